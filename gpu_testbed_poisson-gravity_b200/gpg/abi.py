@@ -1,0 +1,110 @@
+"""ctypes mirror of include/gpg.h (the library's C-ABI) and parameter helpers."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+GPG_OK = 0
+GPG_ERR_INVALID = 1
+GPG_ERR_CUDA = 2
+GPG_ERR_NO_DEVICE = 3
+GPG_ERR_OOM = 4
+GPG_ERR_UNSUPPORTED = 5
+GPG_ERR_STATE = 6
+
+GPG_SOR, GPG_MG = 1, 2
+GPG_INT_CQUAD, GPG_INT_QUAD = 4, 5
+GPG_INIT_INTERP, GPG_INIT_ZERO, GPG_INIT_GUESS = 0, 1, 2
+GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE = 0, 1
+NULL_INT = 2147483647
+
+
+class GpgParams(C.Structure):
+    """Field-for-field copy of ``struct gpg_params`` in include/gpg.h."""
+
+    _fields_ = [
+        ("real_size", C.c_int32),
+        ("ghost", C.c_int32),
+        ("gra_ghost", C.c_int32),
+        ("scheme", C.c_int32),
+        ("int_scheme", C.c_int32),
+        ("p5_gradient", C.c_int32),
+        ("poisson", C.c_int32),
+        ("gra_acc", C.c_int32),
+        ("dt", C.c_double),
+        ("dh", C.c_double),
+        ("sor_min_iter", C.c_int32),
+        ("sor_max_iter", C.c_int32),
+        ("sor_omega", C.c_double),
+        ("mg_max_iter", C.c_int32),
+        ("mg_npre_smooth", C.c_int32),
+        ("mg_npost_smooth", C.c_int32),
+        ("init_mode", C.c_int32),
+        ("mg_tolerated_error", C.c_double),
+        ("poi_coeff", C.c_double),
+        ("stop_mode", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("sor_tolerance", C.c_double),
+    ]
+
+    def copy(self, **kw) -> "GpgParams":
+        p = GpgParams()
+        C.pointer(p)[0] = self
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise AttributeError(k)
+            setattr(p, k, v)
+        return p
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+    @property
+    def dtype(self):
+        import numpy as np
+        return np.float32 if self.real_size == 4 else np.float64
+
+
+SOR_OMEGA = {1: 1.49, 2: 1.57, 3: 1.62, 4: 1.65, 5: 1.69}
+
+
+def default_params(real_size: int = 4, ghost: int = 1, scheme: int = GPG_SOR, **kw) -> GpgParams:
+    """Reference defaults (Main.cpp:1142-1223, Makefile:41-48) in Python;
+    identical to gpg_default_params() of the C library."""
+    if real_size not in (4, 8):
+        raise ValueError("real_size must be 4 or 8")
+    p = GpgParams()
+    p.real_size = real_size
+    p.ghost = ghost
+    p.gra_ghost = 1
+    p.scheme = scheme
+    p.int_scheme = GPG_INT_CQUAD
+    p.p5_gradient = 0
+    p.poisson = 1
+    p.gra_acc = 1
+    p.dt = 1.0e-2
+    p.dh = 1.0
+    p.sor_min_iter = 10
+    p.sor_max_iter = 60 if real_size == 4 else 100
+    p.sor_omega = SOR_OMEGA[ghost]
+    p.mg_max_iter = 10 if real_size == 4 else 20
+    p.mg_npre_smooth = 3
+    p.mg_npost_smooth = 3
+    p.init_mode = GPG_INIT_INTERP
+    p.mg_tolerated_error = 1.0e-6 if real_size == 4 else 1.0e-15
+    p.poi_coeff = 4.0 * math.pi * 1.0e-5
+    p.stop_mode = GPG_STOP_REFERENCE
+    p.reserved0 = 0
+    p.sor_tolerance = 0.0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def patch_sizes(p: GpgParams) -> dict:
+    g, G = p.ghost, p.gra_ghost
+    m = 8 + 2 * (g - 1)
+    pn = 4 + 2 * ((g + 3) // 2)
+    gn = 8 + 2 * G
+    return {"rho": m ** 3, "pot_in": pn ** 3, "pot_out": gn ** 3, "flu": 5 * 512,
+            "rho_nxt": m, "pot_nxt": pn, "gra_nxt": gn, "cube": 8 + 2 * g}

@@ -1,0 +1,163 @@
+/*
+ * gpg.h -- C-ABI of the B200 per-patch Poisson-gravity library (libgpg.so).
+ *
+ * The library replaces the reference testbed's GPU_API/ and GPU_Solver/
+ * (gamer-project/gpu_testbed_poisson-gravity).  Every entry point takes plain
+ * pointers and sizes, returns an int status (GPG_OK == 0) and never exits the
+ * process; gpg_last_error() returns the message of the last failure on the
+ * calling thread.
+ *
+ * Array layouts are the reference's (Header/Prototype.h:6-35), C order, x fastest:
+ *   rho     [P][RHO_NXT][RHO_NXT][RHO_NXT]       RHO_NXT = 8 + 2*(ghost-1)
+ *   pot_in  [P][POT_NXT][POT_NXT][POT_NXT]       POT_NXT = 4 + 2*((ghost+3)/2)
+ *   pot_out [P][GRA_NXT][GRA_NXT][GRA_NXT]       GRA_NXT = 8 + 2*gra_ghost
+ *   flu     [P][5][8][8][8]                      density, px, py, pz, energy
+ * with P = 8 * NPatchGroup in the reference-shaped calls.  Element type is
+ * float when params.real_size == 4 and double when it is 8 (the reference's
+ * `real`, Header/Macro.h:35-39).
+ */
+#ifndef GPG_H
+#define GPG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPG_NULL_INT 2147483647 /* NULL_INT, Header/Macro.h:73-75 */
+#define GPG_ABI_VERSION 1
+
+typedef enum gpg_status {
+  GPG_OK = 0,
+  GPG_ERR_INVALID = 1,     /* bad argument (sizes, schemes, null pointers) */
+  GPG_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  GPG_ERR_NO_DEVICE = 3,   /* no CUDA device / device id out of range */
+  GPG_ERR_OOM = 4,         /* device or pinned host allocation failed */
+  GPG_ERR_UNSUPPORTED = 5, /* valid request this build does not implement */
+  GPG_ERR_STATE = 6        /* call out of order (e.g. solve before allocate) */
+} gpg_status;
+
+/* Poisson schemes, Header/Macro.h:11-14. */
+enum { GPG_SOR = 1, GPG_MG = 2 };
+/* Interpolation schemes, Header/Typedef.h:7-8 (only CQUAD and QUAD exist). */
+enum { GPG_INT_CQUAD = 4, GPG_INT_QUAD = 5 };
+/* SOR initial guess for the patch interior.
+ *   INTERP: interpolated coarse potential (the reference, CPU_PoissonSolver_SOR.cpp:80-209)
+ *   ZERO:   zero interior, interpolated ghost shell
+ *   GUESS:  interior taken from a caller array [P][RHO_NXT]^3 */
+enum { GPG_INIT_INTERP = 0, GPG_INIT_ZERO = 1, GPG_INIT_GUESS = 2 };
+/* SOR stopping rule.
+ *   REFERENCE: stop after the first sweep whose L1 residual grows, once
+ *              Iter+1 >= Min_Iter; cap Max_Iter (CPU_PoissonSolver_SOR.cpp:273-283)
+ *   TOLERANCE: stop once Iter+1 >= Min_Iter and the sweep's L1 residual
+ *              <= sor_tolerance * sum|Poi_Coeff*dh^2*rho|; cap Max_Iter */
+enum { GPG_STOP_REFERENCE = 0, GPG_STOP_TOLERANCE = 1 };
+
+/* Runtime form of the reference's compile-time shape (Makefile:13-85) plus the
+ * argument list of CUAPI_Asyn_PoissonGravitySolver (Header/Prototype.h:25-34).
+ * Fields are converted to `real` exactly where the reference converts them. */
+typedef struct gpg_params {
+  int32_t real_size;       /* 4 or 8 */
+  int32_t ghost;           /* POT_GHOST_SIZE, 1..5 */
+  int32_t gra_ghost;       /* GRA_GHOST_SIZE, 0..2, <= ghost */
+  int32_t scheme;          /* GPG_SOR | GPG_MG */
+  int32_t int_scheme;      /* GPG_INT_CQUAD | GPG_INT_QUAD */
+  int32_t p5_gradient;     /* 5-point gradient; needs gra_ghost == 2 */
+  int32_t poisson;         /* run the Poisson solver */
+  int32_t gra_acc;         /* run the gravity update */
+  double dt;
+  double dh;
+  int32_t sor_min_iter;
+  int32_t sor_max_iter;
+  double sor_omega;
+  int32_t mg_max_iter;
+  int32_t mg_npre_smooth;
+  int32_t mg_npost_smooth;
+  int32_t init_mode;       /* GPG_INIT_* (SOR only) */
+  double mg_tolerated_error;
+  double poi_coeff;        /* 4*pi*G*a */
+  int32_t stop_mode;       /* GPG_STOP_* (SOR only) */
+  int32_t reserved0;
+  double sor_tolerance;    /* relative L1 tolerance for GPG_STOP_TOLERANCE */
+} gpg_params;
+
+/* Fill `p` with the reference defaults for (real_size, ghost, scheme):
+ * omega / Min_Iter / Max_Iter of Main.cpp:1142-1157, MG settings of
+ * Main.cpp:1173-1223, dt = 1e-2, dh = 1, Poi_Coeff = 4*pi*1e-5, CQUAD,
+ * gra_ghost = 1, Poisson and GraAcc on. */
+int gpg_default_params(gpg_params *p, int real_size, int ghost, int scheme);
+
+/* Check a parameter block (same checks as CUAPI_Asyn_PoissonGravitySolver.cu:116-140). */
+int gpg_validate_params(const gpg_params *p);
+
+/* Element counts per patch of each array for the shape in `p`. */
+int gpg_patch_sizes(const gpg_params *p, int64_t *rho, int64_t *pot_in, int64_t *pot_out,
+                    int64_t *flu);
+
+const char *gpg_last_error(void);
+int gpg_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Stream-ordered device API.  All pointers are device pointers the caller owns;
+ * the call only enqueues work on `stream` (a cudaStream_t, NULL = legacy default).
+ *   d_guess  : [P][RHO_NXT]^3, read when init_mode == GPG_INIT_GUESS, else may be NULL
+ *   d_iters  : [P] int32, per-patch SOR sweeps / MG V-cycles (may be NULL)
+ *   d_resid  : [P] double, final SOR L1 residual / MG error estimate (may be NULL)
+ * Replaces the kernel launches of CUAPI_Asyn_PoissonGravitySolver.cu:204-249
+ * (CUPOT_PoissonSolver_SOR_10to14cube / _16to18cube / _MG and CUPOT_GravitySolver).
+ * With poisson && gra_acc the gravity update is fused into the Poisson kernel
+ * (one launch); with only gra_acc, d_pot_out is the input potential.
+ * ------------------------------------------------------------------------- */
+int gpg_poisson_gravity_device(const gpg_params *p, int npatch, const void *d_rho,
+                               const void *d_pot_in, void *d_pot_out, void *d_flu,
+                               const void *d_guess, int32_t *d_iters, double *d_resid,
+                               void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Reference-shaped host API (Header/Prototype.h:15-35).  One context holds the
+ * device buffers, pinned host buffers and streams that the reference keeps in
+ * module globals (GPU_API/CUAPI_Asyn_PoissonGravitySolver.cu:32-39).
+ * ------------------------------------------------------------------------- */
+typedef struct gpg_context gpg_context;
+
+/* CUAPI_Set_Diagnose_Device (GPU_API/CUAPI_Set_Diagnose_Device.cu:45-292):
+ * select the device and replace GPG_NULL_INT in *npgroup / *nstream with
+ * defaults (streams: 4; patch groups: 32 * SM count). */
+int gpg_set_diagnose_device(int *npgroup, int *nstream, int device_id);
+
+int gpg_context_create(gpg_context **ctx, int device_id, int nstream);
+int gpg_context_destroy(gpg_context *ctx);
+
+/* CUAPI_MemAllocate_PoissonGravity (GPU_API/CUAPI_MemAllocate_PoissonGravity.cu:27-80):
+ * device buffers for npatch_group*8 patches of the shape in `shape`, plus pinned
+ * host buffers returned through the four out-pointers. */
+int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int npatch_group,
+                     void **h_rho, void **h_pot_in, void **h_pot_out, void **h_flu);
+
+/* CUAPI_MemFree_PoissonGravity (GPU_API/CUAPI_MemFree_PoissonGravity.cu:27-70). */
+int gpg_mem_free(gpg_context *ctx, void **h_rho, void **h_pot_in, void **h_pot_out,
+                 void **h_flu);
+
+/* CUAPI_Asyn_PoissonGravitySolver (GPU_API/CUAPI_Asyn_PoissonGravitySolver.cu:85-275):
+ * per stream, H2D of rho / pot_in (and pot_out when !poisson) / flu, the solve,
+ * D2H of pot_out / flu.  Returns before the GPU finishes; call gpg_synchronize()
+ * before reading h_pot_out / h_flu.  h_flu is in/out. */
+int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_rho, void *h_pot_in,
+                                    void *h_pot_out, void *h_flu, int npatch_group,
+                                    const gpg_params *p, int nstream);
+
+/* CUAPI_Synchronize (GPU_API/CUAPI_Synchronize.cu:10-13). */
+int gpg_synchronize(gpg_context *ctx);
+
+/* Per-patch iteration counts / residuals of the last completed solve (host
+ * copies; valid after gpg_synchronize).  No reference counterpart: the
+ * reference only prints them (CPU_PoissonSolver_SOR.cpp:288). */
+int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPG_H */
