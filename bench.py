@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the per-patch Poisson(-gravity) hot path on B200.
+
+Workload (one "step"): plain red-black SOR with the reference's parameters and
+convergence rule (interpolated start, stop when the L1 residual grows after
+Min_Iter = 10, Max_Iter 60 / 100) over ghost sizes 2, 3, 4, 5 with 4096
+patches each, in FP32 and in FP64 -- 8 batches, 32768 patches per step per GPU.
+Inputs: seeded power-law density rho = (r/8)^-2 (1 + 0.05 N(0,1)) in a 16^3-
+patch box and the matching analytic coarse potential (gpg.inputs).
+
+Reported (one JSON line from rank 0):
+  value      patches/s over the whole job, inputs resident in HBM (device timing,
+             CUDA events on the launching stream, max over ranks)
+  e2e        the same through the reference-shaped host API (pinned host
+             buffers, H2D + solve + D2H per step; host clock around a full sync)
+  roofline   dominant kernel: compulsory HBM bytes per launch / mean launch time
+  cpu_baseline  the reference's own CPU code (oracle/_ref, all host threads) on
+             a bounded sample of the same workload
+`--impl reference` runs only the reference CPU path (rank 0) and prints its line.
+Multi-GPU (torchrun): every rank solves its own 32768 patches (weak scaling, no
+collective in the solve); only the timing max goes through the process group.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "gpu_testbed_poisson-gravity_b200"))
+
+from gpg.abi import GPG_SOR, default_params, patch_sizes  # noqa: E402
+from gpg.inputs import make_patches  # noqa: E402
+
+METRIC = "patches/s to fixed residual on 1 B200: learned-init+SOR vs plain SOR"
+GHOSTS = (2, 3, 4, 5)
+PRECS = (4, 8)
+NPATCH = 4096
+L2_BYTES = 126 * 2 ** 20
+
+
+def workload(rank: int):
+    """[(params, inputs)] for the 8 batches of one step on this rank."""
+    out = []
+    for rs in PRECS:
+        for g in GHOSTS:
+            p = default_params(rs, g, GPG_SOR, gra_acc=0)
+            dt = np.float32 if rs == 4 else np.float64
+            d = make_patches(NPATCH, g, seed=1000 * (rank + 1) + g, dtype=dt, fluid=False)
+            out.append((p, d))
+    return out
+
+
+def compulsory_bytes(p) -> int:
+    s = patch_sizes(p)
+    return (s["rho"] + s["pot_in"] + s["pot_out"]) * p.real_size
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+        if not rows:
+            return None
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for _, _, flags in rows for n, fl in zip(names, flags) if fl.lower() == "active"})
+        sm = sorted(r[0] for r in rows)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path
+# ---------------------------------------------------------------------------
+def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0):
+    """Time the reference's CPU_PoissonGravitySolver (oracle/_ref; the C port
+    of oracle/ when the reference objects are absent) on a bounded sample of
+    every batch.  Returns (patches/s, cores, kind, sample description)."""
+    from oracle.oracle import oracle_lib, ref_available, run_oracle, run_reference
+    kind = "reference" if all(ref_available("sor", p.ghost, 1, "f32" if p.real_size == 4 else "f64")
+                              for p, _ in batches) else "port"
+    cores = nthreads or (oracle_lib().oracle_max_threads())
+    # per batch sample: first n patches (multiple of 8), sized from a probe run
+    total_t, total_p, desc = 0.0, 0, []
+    per_batch = budget_s / len(batches)
+    for p, d in batches:
+        n = 64
+        while True:
+            t0 = time.perf_counter()
+            _run_cpu(kind, p, d, n, nthreads)
+            dt = time.perf_counter() - t0
+            if dt > per_batch / 4 or n >= len(d["rho"]):
+                break
+            n = min(len(d["rho"]), n * 4)
+        t0 = time.perf_counter()
+        _run_cpu(kind, p, d, n, nthreads)
+        dt = time.perf_counter() - t0
+        total_t += dt
+        total_p += n
+        desc.append(f"g{p.ghost}/f{8 * p.real_size}:{n}")
+    return total_p / total_t, cores, kind, "patches per batch " + ",".join(desc)
+
+
+def _run_cpu(kind, p, d, n, nthreads):
+    from oracle.oracle import run_oracle, run_reference
+    rho = np.ascontiguousarray(d["rho"][:n])
+    pin = np.ascontiguousarray(d["pot_in"][:n])
+    if kind == "reference":
+        q = p.copy(gra_acc=0)
+        run_reference(q, rho, pin.copy(), nthreads=nthreads)
+    else:
+        run_oracle(p, rho, pin, accum_f64=False, nthreads=nthreads)
+
+
+# ---------------------------------------------------------------------------
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    a = ap.parse_args(argv)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        batches = workload(0)
+        t_all = []
+        for _ in range(a.warmup):
+            reference_cpu(batches, budget_s=2.0)
+        vals = []
+        for _ in range(a.steps):
+            v, cores, kind, sample = reference_cpu(batches, budget_s=8.0)
+            vals.append(v)
+        v = float(np.median(vals))
+        line = {"metric": METRIC, "value": v, "unit": "patches/s", "n_gpus": a.gpus, "steps": a.steps,
+                "warmup": a.warmup, "higher_is_better": True, "impl": "reference",
+                "dtype": "f32+f64", "data": "synthetic",
+                "config": {"workload": "plain SOR, reference rule, ghost 2-5 x 4096 patches, FP32+FP64",
+                           "global_batch": len(batches) * NPATCH},
+                "cpu_baseline": {"value": v, "unit": "patches/s", "cores": cores, "kind": kind,
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "vs_baseline": None}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    from gpg.lib import Context, library, solve_device
+    library()
+
+    batches = workload(rank)
+    dev_in = []
+    for p, d in batches:
+        n = len(d["rho"])
+        gn = 8 + 2 * p.gra_ghost
+        tdt = torch.float32 if p.real_size == 4 else torch.float64
+        dev_in.append(dict(rho=torch.from_numpy(d["rho"]).to(dev), pot_in=torch.from_numpy(d["pot_in"]).to(dev),
+                           pot_out=torch.empty((n, gn, gn, gn), dtype=tdt, device=dev),
+                           iters=torch.empty(n, dtype=torch.int32, device=dev),
+                           resid=torch.empty(n, dtype=torch.float64, device=dev)))
+    stream = torch.cuda.current_stream(dev)
+    step_inputs = sum((d["rho"].nbytes + d["pot_in"].nbytes) for _, d in batches)
+
+    def step(events=None):
+        for k, ((p, _), t) in enumerate(zip(batches, dev_in)):
+            if events is not None:
+                events[k][0].record(stream)
+            solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], iters=t["iters"], resid=t["resid"])
+            if events is not None:
+                events[k][1].record(stream)
+
+    for _ in range(max(a.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in batches]
+          for _ in range(a.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        barrier()
+        start.record(stream)
+        for s in range(a.steps):
+            step(ev[s])
+        stop.record(stream)
+        barrier()
+    ms = start.elapsed_time(stop)
+    per_kernel = np.array([[e[0].elapsed_time(e[1]) for e in row] for row in ev])  # [steps, batches]
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    patches_step = NPATCH * len(batches)
+    value = world * patches_step * a.steps / (ms / 1e3)
+    iters = [t["iters"].cpu().numpy() for t in dev_in]
+
+    # ---- end to end through the reference-shaped host API ----------------
+    e2e = None
+    if not a.no_e2e:
+        ctxs = []
+        for (p, d) in batches:
+            c = Context(dev.index, nstream=4)
+            rho, pin, pout, _ = c.allocate(p, NPATCH // 8)
+            rho[...] = d["rho"]
+            pin[...] = d["pot_in"]
+            ctxs.append(c)
+        for _ in range(2):
+            for (p, _), c in zip(batches, ctxs):
+                c.asyn_solve(p, NPATCH // 8)
+            for c in ctxs:
+                c.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            for (p, _), c in zip(batches, ctxs):
+                c.asyn_solve(p, NPATCH // 8)
+            for c in ctxs:
+                c.synchronize()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = step_inputs
+        d2h = sum(NPATCH * (patch_sizes(p)["pot_out"] * p.real_size + 4 + 8) for p, _ in batches)
+        e2e = {"value": world * patches_step * a.steps / e2e_s, "unit": "patches/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "timing": "host clock around full device sync"}
+        for c in ctxs:
+            c.close()
+
+    # ---- roofline of the dominant kernel ---------------------------------
+    tot = per_kernel.sum(0)
+    k = int(np.argmax(tot))
+    pk, _ = batches[k]
+    launch_ms = float(per_kernel[:, k].mean())
+    algo_bytes = compulsory_bytes(pk) * NPATCH
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = algo_bytes / (launch_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as f:
+            tr = json.load(f)
+        traffic = tr.get(f"sor_f{8 * pk.real_size}_g{pk.ghost}_{NPATCH}")
+    except OSError:
+        pass
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "patches/s", "n_gpus": world, "steps": a.steps,
+        "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "plain SOR, reference rule (interpolated start, stop on residual growth, "
+                               "Min 10 / Max 60|100), ghost 2-5 x 4096 patches, FP32+FP64, Poisson only",
+                   "global_batch": world * patches_step, "patches_per_gpu": patches_step,
+                   "l2": f"step inputs {step_inputs / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
+                   "parallelism": f"patch shards x{world}", "learned_init": "not built"},
+        "gpu_launches": len(batches) * a.steps,
+        "per_batch_ms": {f"f{8 * p.real_size}_g{p.ghost}": float(per_kernel[:, i].mean())
+                         for i, (p, _) in enumerate(batches)},
+        "mean_iters": {f"f{8 * p.real_size}_g{p.ghost}": float(it.mean()) for (p, _), it in zip(batches, iters)},
+        "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
+                     "launch_ms": launch_ms, "peak_source": "measured" if peaks else "fallback"},
+        "e2e": e2e,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not a.no_cpu_baseline and world == 1:
+        v, cores, kind, sample = reference_cpu(batches, budget_s=20.0)
+        line["cpu_baseline"] = {"value": v, "unit": "patches/s", "cores": cores, "kind": kind, "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,521 @@
+// gpg_api.cu -- C-ABI of libgpg (include/gpg.h): parameter handling, kernel
+// dispatch, and the reference-shaped context API (device buffers, pinned host
+// buffers, streams) that replaces GPU_API/CUAPI_*.cu.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gpg.h"
+#include "gravity.cuh"
+#include "mg_kernel.cuh"
+#include "sor_kernel.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+#define GPG_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(e_ == cudaErrorMemoryAllocation ? GPG_ERR_OOM : GPG_ERR_CUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// launch configuration per (precision, ghost size)
+// ---------------------------------------------------------------------------
+// SOR teams per CTA: aim for 128-thread CTAs (teams of 32/64/96/128/128 threads).
+template <int G> constexpr int sor_ppc() { return G == 1 ? 4 : (G == 2 ? 2 : 1); }
+// MG threads per CTA (one patch per CTA).
+template <int G> constexpr int mg_threads() { return G <= 2 ? 128 : 256; }
+
+template <typename KernelFn>
+int ensure_smem(KernelFn *fn, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess)
+      return fail(GPG_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  return GPG_OK;
+}
+
+template <typename T, int G>
+int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  constexpr int PPC = sor_ppc<G>();
+  using S = gpg::SorSmem<T, G>;
+  const size_t smem = PPC * S::team_bytes;
+  auto fn = gpg::sor_kernel<T, G, PPC>;
+  if (int rc = ensure_smem(fn, smem)) return rc;
+  const int64_t grid = (a.npatch + PPC - 1) / PPC;
+  fn<<<(unsigned)grid, PPC * gpg::Geo<G>::TEAM, smem, s>>>(a);
+  GPG_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+template <typename T, int G>
+int launch_mg(const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  constexpr int NT = mg_threads<G>();
+  const size_t smem = gpg::MgSmem<T, G, NT>::bytes;
+  auto fn = gpg::mg_kernel<T, G, NT>;
+  if (int rc = ensure_smem(fn, smem)) return rc;
+  fn<<<(unsigned)a.npatch, NT, smem, s>>>(a);
+  GPG_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+template <typename T, int GG>
+int launch_gravity(const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  gpg::gravity_kernel<T, GG><<<(unsigned)a.npatch, 256, 0, s>>>(a.flu, a.pot_out, a.npatch, a.gra_const, a.p5);
+  GPG_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+template <typename T>
+gpg::SolveArgs<T> make_args(const gpg_params &p, int64_t npatch, const void *rho, const void *pin, void *pout,
+                            void *flu, const void *guess, int32_t *iters, double *resid) {
+  gpg::SolveArgs<T> a{};
+  a.rho = static_cast<const T *>(rho);
+  a.pot_in = static_cast<const T *>(pin);
+  a.pot_out = static_cast<T *>(pout);
+  a.flu = static_cast<T *>(flu);
+  a.guess = static_cast<const T *>(guess);
+  a.iters = iters;
+  a.resid = resid;
+  a.npatch = npatch;
+  // rounding exactly where the reference rounds: its CPU_* functions take
+  // `real` arguments and form these constants in `real`
+  // (CPU_PoissonSolver_SOR.cpp:51-52, CPU_GravitySolver.cpp:23)
+  const T dh = (T)p.dh, dt = (T)p.dt, poi = (T)p.poi_coeff, omega = (T)p.sor_omega;
+  volatile T c = poi;  // volatile: keep each product rounded to T on the host
+  c = c * dh;
+  c = c * dh;
+  a.sor_const = c;
+  volatile T o6 = omega;
+  o6 = o6 / (T)6.0;
+  a.omega_6 = o6;
+  a.gra_const = p.p5_gradient ? (T)((double)dt / (12.0 * (double)dh)) : (T)((double)dt / (2.0 * (double)dh));
+  a.dh = dh;
+  a.poi_coeff = poi;
+  a.mg_tol = (T)p.mg_tolerated_error;
+  a.sor_tol = p.sor_tolerance;
+  a.min_iter = p.sor_min_iter;
+  a.max_iter = p.sor_max_iter;
+  a.mg_max_iter = p.mg_max_iter;
+  a.mg_npre = p.mg_npre_smooth;
+  a.mg_npost = p.mg_npost_smooth;
+  a.int_scheme = p.int_scheme;
+  a.init_mode = p.init_mode;
+  a.stop_mode = p.stop_mode;
+  a.gra_ghost = p.gra_ghost;
+  a.gra_acc = p.gra_acc;
+  a.p5 = p.p5_gradient;
+  return a;
+}
+
+template <typename T>
+int solve_typed(const gpg_params &p, int64_t npatch, const void *rho, const void *pin, void *pout, void *flu,
+                const void *guess, int32_t *iters, double *resid, cudaStream_t s) {
+  auto a = make_args<T>(p, npatch, rho, pin, pout, flu, guess, iters, resid);
+  if (p.poisson) {
+    // the fused kernel applies gravity itself when gra_acc is set
+    if (p.scheme == GPG_SOR) {
+      switch (p.ghost) {
+        case 1: return launch_sor<T, 1>(a, s);
+        case 2: return launch_sor<T, 2>(a, s);
+        case 3: return launch_sor<T, 3>(a, s);
+        case 4: return launch_sor<T, 4>(a, s);
+        case 5: return launch_sor<T, 5>(a, s);
+      }
+    } else {
+      switch (p.ghost) {
+        case 1: return launch_mg<T, 1>(a, s);
+        case 2: return launch_mg<T, 2>(a, s);
+        case 3: return launch_mg<T, 3>(a, s);
+        case 4: return launch_mg<T, 4>(a, s);
+        case 5: return launch_mg<T, 5>(a, s);
+      }
+    }
+    return fail(GPG_ERR_INVALID, "ghost %d", p.ghost);
+  }
+  if (p.gra_acc) {
+    switch (p.gra_ghost) {
+      case 1: return launch_gravity<T, 1>(a, s);
+      case 2: return launch_gravity<T, 2>(a, s);
+    }
+  }
+  return GPG_OK;
+}
+
+int check_ptr(const void *ptr, const char *name) {
+  if (ptr == nullptr) return fail(GPG_ERR_INVALID, "%s is NULL", name);
+  return GPG_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// parameters
+// ===========================================================================
+extern "C" int gpg_abi_version(void) { return GPG_ABI_VERSION; }
+
+extern "C" const char *gpg_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int gpg_default_params(gpg_params *p, int real_size, int ghost, int scheme) {
+  if (!p) return fail(GPG_ERR_INVALID, "params is NULL");
+  if (real_size != 4 && real_size != 8) return fail(GPG_ERR_INVALID, "real_size %d (must be 4 or 8)", real_size);
+  if (ghost < 1 || ghost > 5) return fail(GPG_ERR_INVALID, "ghost %d (must be 1..5)", ghost);
+  if (scheme != GPG_SOR && scheme != GPG_MG) return fail(GPG_ERR_INVALID, "scheme %d", scheme);
+  static const double omega[5] = {1.49, 1.57, 1.62, 1.65, 1.69};  // Main.cpp:1145
+  std::memset(p, 0, sizeof *p);
+  p->real_size = real_size;
+  p->ghost = ghost;
+  p->gra_ghost = 1;
+  p->scheme = scheme;
+  p->int_scheme = GPG_INT_CQUAD;
+  p->p5_gradient = 0;
+  p->poisson = 1;
+  p->gra_acc = 1;
+  p->dt = 1.0e-2;
+  p->dh = 1.0;
+  p->sor_min_iter = 10;
+  p->sor_max_iter = real_size == 4 ? 60 : 100;
+  p->sor_omega = omega[ghost - 1];
+  p->mg_max_iter = real_size == 4 ? 10 : 20;
+  p->mg_npre_smooth = 3;
+  p->mg_npost_smooth = 3;
+  p->init_mode = GPG_INIT_INTERP;
+  p->mg_tolerated_error = real_size == 4 ? 1.0e-6 : 1.0e-15;
+  p->poi_coeff = 4.0 * M_PI * 1.0e-5;
+  p->stop_mode = GPG_STOP_REFERENCE;
+  p->sor_tolerance = 0.0;
+  return GPG_OK;
+}
+
+extern "C" int gpg_validate_params(const gpg_params *p) {
+  if (!p) return fail(GPG_ERR_INVALID, "params is NULL");
+  if (p->real_size != 4 && p->real_size != 8) return fail(GPG_ERR_INVALID, "real_size %d", p->real_size);
+  if (p->ghost < 1 || p->ghost > 5) return fail(GPG_ERR_INVALID, "ghost %d (must be 1..5)", p->ghost);
+  if (p->gra_ghost < 0 || p->gra_ghost > 2 || p->gra_ghost > p->ghost)
+    return fail(GPG_ERR_INVALID, "gra_ghost %d (must be 0..2 and <= ghost %d)", p->gra_ghost, p->ghost);
+  if (p->poisson) {
+    if (p->scheme != GPG_SOR && p->scheme != GPG_MG) return fail(GPG_ERR_INVALID, "scheme %d", p->scheme);
+    // CUAPI_Asyn_PoissonGravitySolver.cu:134-135
+    if (p->int_scheme != GPG_INT_CQUAD && p->int_scheme != GPG_INT_QUAD)
+      return fail(GPG_ERR_INVALID, "incorrect parameter IntScheme = %d", p->int_scheme);
+    if (p->scheme == GPG_SOR) {
+      if (p->sor_max_iter < 0) return fail(GPG_ERR_INVALID, "sor_max_iter %d", p->sor_max_iter);
+      if (p->init_mode < 0 || p->init_mode > 2) return fail(GPG_ERR_INVALID, "init_mode %d", p->init_mode);
+      if (p->stop_mode < 0 || p->stop_mode > 1) return fail(GPG_ERR_INVALID, "stop_mode %d", p->stop_mode);
+      if (p->stop_mode == GPG_STOP_TOLERANCE && !(p->sor_tolerance >= 0.0))
+        return fail(GPG_ERR_INVALID, "sor_tolerance %g", p->sor_tolerance);
+    } else {
+      if (p->mg_max_iter < 0 || p->mg_npre_smooth < 0 || p->mg_npost_smooth < 0)
+        return fail(GPG_ERR_INVALID, "negative MG parameter");
+    }
+  }
+  if (p->gra_acc) {
+    if (p->gra_ghost < 1) return fail(GPG_ERR_INVALID, "gravity needs gra_ghost >= 1");
+    // CUAPI_Asyn_PoissonGravitySolver.cu:137-140
+    if (p->p5_gradient && p->gra_ghost != 2)
+      return fail(GPG_ERR_INVALID, "incorrect parameter P5_Gradient = %d (needs gra_ghost 2)", p->p5_gradient);
+  }
+  return GPG_OK;
+}
+
+extern "C" int gpg_patch_sizes(const gpg_params *p, int64_t *rho, int64_t *pot_in, int64_t *pot_out, int64_t *flu) {
+  if (!p) return fail(GPG_ERR_INVALID, "params is NULL");
+  const int g = p->ghost, G = p->gra_ghost;
+  if (g < 1 || g > 5 || G < 0 || G > 2) return fail(GPG_ERR_INVALID, "ghost %d / gra_ghost %d", g, G);
+  const int64_t m = 8 + 2 * (g - 1), pn = 4 + 2 * ((g + 3) / 2), gn = 8 + 2 * G;
+  if (rho) *rho = m * m * m;
+  if (pot_in) *pot_in = pn * pn * pn;
+  if (pot_out) *pot_out = gn * gn * gn;
+  if (flu) *flu = 5 * 512;
+  return GPG_OK;
+}
+
+// ===========================================================================
+// stream-ordered device API
+// ===========================================================================
+extern "C" int gpg_poisson_gravity_device(const gpg_params *p, int npatch, const void *d_rho, const void *d_pot_in,
+                                          void *d_pot_out, void *d_flu, const void *d_guess, int32_t *d_iters,
+                                          double *d_resid, void *stream) {
+  if (int rc = gpg_validate_params(p)) return rc;
+  if (npatch < 0) return fail(GPG_ERR_INVALID, "npatch %d", npatch);
+  if (npatch == 0) return GPG_OK;
+  if (p->poisson) {
+    if (int rc = check_ptr(d_rho, "d_rho")) return rc;
+    if (int rc = check_ptr(d_pot_in, "d_pot_in")) return rc;
+    if (p->scheme == GPG_SOR && p->init_mode == GPG_INIT_GUESS)
+      if (int rc = check_ptr(d_guess, "d_guess")) return rc;
+  }
+  if (p->poisson || p->gra_acc)
+    if (int rc = check_ptr(d_pot_out, "d_pot_out")) return rc;
+  if (p->gra_acc)
+    if (int rc = check_ptr(d_flu, "d_flu")) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->real_size == 4)
+    return solve_typed<float>(*p, npatch, d_rho, d_pot_in, d_pot_out, d_flu, d_guess, d_iters, d_resid, s);
+  return solve_typed<double>(*p, npatch, d_rho, d_pot_in, d_pot_out, d_flu, d_guess, d_iters, d_resid, s);
+}
+
+// ===========================================================================
+// reference-shaped context API
+// ===========================================================================
+struct gpg_context {
+  int device = 0;
+  int nstream = 1;
+  std::vector<cudaStream_t> streams;
+  gpg_params shape{};
+  int64_t cap = 0;  // patches the buffers hold
+  int64_t n_rho = 0, n_pin = 0, n_pout = 0, n_flu = 0;
+  void *d_rho = nullptr, *d_pin = nullptr, *d_pout = nullptr, *d_flu = nullptr;
+  int32_t *d_iters = nullptr;
+  double *d_resid = nullptr;
+  void *h_rho = nullptr, *h_pin = nullptr, *h_pout = nullptr, *h_flu = nullptr;
+  int32_t *h_iters = nullptr;
+  double *h_resid = nullptr;
+  int64_t last_npatch = 0;
+};
+
+extern "C" int gpg_set_diagnose_device(int *npgroup, int *nstream, int device_id) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(GPG_ERR_NO_DEVICE, "no devices supporting CUDA (%s)", cudaGetErrorString(e));
+  if (device_id < 0 || device_id >= count)
+    return fail(GPG_ERR_NO_DEVICE, "Input GPU ID (%d) >= # of GPUs (%d)", device_id, count);
+  GPG_CUDA(cudaSetDevice(device_id));
+  cudaDeviceProp prop;
+  GPG_CUDA(cudaGetDeviceProperties(&prop, device_id));
+  if (prop.major != 10 || prop.minor != 0)
+    return fail(GPG_ERR_UNSUPPORTED, "device \"%s\" is sm_%d%d; this library is built for sm_100a", prop.name,
+                prop.major, prop.minor);
+  if (nstream && *nstream == GPG_NULL_INT) *nstream = 4;
+  if (npgroup && *npgroup == GPG_NULL_INT) *npgroup = 32 * prop.multiProcessorCount;
+  return GPG_OK;
+}
+
+extern "C" int gpg_context_create(gpg_context **out, int device_id, int nstream) {
+  if (!out) return fail(GPG_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (nstream < 1 || nstream > 1024) return fail(GPG_ERR_INVALID, "nstream %d", nstream);
+  int ns = nstream, npg = 1;
+  if (int rc = gpg_set_diagnose_device(&npg, &ns, device_id)) return rc;
+  auto *ctx = new gpg_context;
+  ctx->device = device_id;
+  ctx->nstream = nstream;
+  ctx->streams.resize(nstream);
+  for (int s = 0; s < nstream; ++s) {
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->streams[s], cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      for (int t = 0; t < s; ++t) cudaStreamDestroy(ctx->streams[t]);
+      delete ctx;
+      return fail(GPG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+  }
+  *out = ctx;
+  return GPG_OK;
+}
+
+static void release_buffers(gpg_context *c) {
+  cudaFree(c->d_rho);
+  cudaFree(c->d_pin);
+  cudaFree(c->d_pout);
+  cudaFree(c->d_flu);
+  cudaFree(c->d_iters);
+  cudaFree(c->d_resid);
+  cudaFreeHost(c->h_iters);
+  cudaFreeHost(c->h_resid);
+  c->d_rho = c->d_pin = c->d_pout = c->d_flu = nullptr;
+  c->d_iters = nullptr;
+  c->d_resid = nullptr;
+  c->h_iters = nullptr;
+  c->h_resid = nullptr;
+  c->cap = 0;
+}
+
+extern "C" int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int npatch_group, void **h_rho,
+                                void **h_pot_in, void **h_pot_out, void **h_flu) {
+  if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
+  if (int rc = gpg_validate_params(shape)) return rc;
+  if (npatch_group < 0) return fail(GPG_ERR_INVALID, "npatch_group %d", npatch_group);
+  if (ctx->cap) return fail(GPG_ERR_STATE, "buffers already allocated (call gpg_mem_free first)");
+  GPG_CUDA(cudaSetDevice(ctx->device));
+  ctx->shape = *shape;
+  ctx->cap = 8 * (int64_t)npatch_group;
+  gpg_patch_sizes(shape, &ctx->n_rho, &ctx->n_pin, &ctx->n_pout, &ctx->n_flu);
+  const size_t es = shape->real_size, n = ctx->cap;
+  const size_t b_rho = es * n * ctx->n_rho, b_pin = es * n * ctx->n_pin, b_pout = es * n * ctx->n_pout,
+               b_flu = es * n * ctx->n_flu;
+  auto chk = [&](cudaError_t e, const char *what) -> int {
+    if (e == cudaSuccess) return GPG_OK;
+    release_buffers(ctx);
+    return fail(e == cudaErrorMemoryAllocation ? GPG_ERR_OOM : GPG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  };
+  if (int rc = chk(cudaMalloc(&ctx->d_rho, b_rho), "cudaMalloc rho")) return rc;
+  if (int rc = chk(cudaMalloc(&ctx->d_pin, b_pin), "cudaMalloc pot_in")) return rc;
+  if (int rc = chk(cudaMalloc(&ctx->d_pout, b_pout), "cudaMalloc pot_out")) return rc;
+  if (int rc = chk(cudaMalloc(&ctx->d_flu, b_flu), "cudaMalloc flu")) return rc;
+  if (int rc = chk(cudaMalloc(&ctx->d_iters, sizeof(int32_t) * (n ? n : 1)), "cudaMalloc iters")) return rc;
+  if (int rc = chk(cudaMalloc(&ctx->d_resid, sizeof(double) * (n ? n : 1)), "cudaMalloc resid")) return rc;
+  if (int rc = chk(cudaMallocHost(&ctx->h_iters, sizeof(int32_t) * (n ? n : 1)), "cudaMallocHost iters")) return rc;
+  if (int rc = chk(cudaMallocHost(&ctx->h_resid, sizeof(double) * (n ? n : 1)), "cudaMallocHost resid")) return rc;
+  // pinned host arrays handed to the caller (CUAPI_MemAllocate_PoissonGravity.cu:66-69)
+  void **outs[4] = {h_rho, h_pot_in, h_pot_out, h_flu};
+  const size_t sizes[4] = {b_rho, b_pin, b_pout, b_flu};
+  void *pinned[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int k = 0; k < 4; ++k) {
+    if (!outs[k]) continue;
+    cudaError_t e = cudaMallocHost(&pinned[k], sizes[k] ? sizes[k] : 16);
+    if (e != cudaSuccess) {
+      for (int t = 0; t < k; ++t) cudaFreeHost(pinned[t]);
+      return chk(e, "cudaMallocHost");
+    }
+  }
+  for (int k = 0; k < 4; ++k)
+    if (outs[k]) *outs[k] = pinned[k];
+  return GPG_OK;
+}
+
+extern "C" int gpg_mem_free(gpg_context *ctx, void **h_rho, void **h_pot_in, void **h_pot_out, void **h_flu) {
+  if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
+  GPG_CUDA(cudaSetDevice(ctx->device));
+  for (auto s : ctx->streams) cudaStreamSynchronize(s);
+  release_buffers(ctx);
+  void **outs[4] = {h_rho, h_pot_in, h_pot_out, h_flu};
+  for (int k = 0; k < 4; ++k) {
+    if (outs[k] && *outs[k]) {
+      cudaError_t e = cudaFreeHost(*outs[k]);
+      if (e != cudaSuccess) return fail(GPG_ERR_CUDA, "cudaFreeHost: %s", cudaGetErrorString(e));
+      *outs[k] = nullptr;
+    }
+  }
+  return GPG_OK;
+}
+
+extern "C" int gpg_context_destroy(gpg_context *ctx) {
+  if (!ctx) return GPG_OK;
+  cudaSetDevice(ctx->device);
+  for (auto s : ctx->streams) cudaStreamSynchronize(s);
+  release_buffers(ctx);
+  for (auto s : ctx->streams) cudaStreamDestroy(s);
+  delete ctx;
+  return GPG_OK;
+}
+
+extern "C" int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_rho, void *h_pot_in, void *h_pot_out,
+                                               void *h_flu, int npatch_group, const gpg_params *p, int nstream) {
+  if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
+  if (int rc = gpg_validate_params(p)) return rc;
+  if (!ctx->cap && npatch_group > 0) return fail(GPG_ERR_STATE, "no buffers (call gpg_mem_allocate first)");
+  if (p->real_size != ctx->shape.real_size || p->ghost != ctx->shape.ghost || p->gra_ghost != ctx->shape.gra_ghost)
+    return fail(GPG_ERR_INVALID, "parameters do not match the allocated shape");
+  if (p->poisson && p->init_mode == GPG_INIT_GUESS)
+    return fail(GPG_ERR_UNSUPPORTED, "GPG_INIT_GUESS needs the device API");
+  const int64_t npatch = 8 * (int64_t)npatch_group;
+  if (npatch_group < 0 || npatch > ctx->cap)
+    return fail(GPG_ERR_INVALID, "npatch_group %d exceeds the allocated %lld patches", npatch_group,
+                (long long)ctx->cap);
+  if (nstream < 1 || nstream > ctx->nstream)
+    return fail(GPG_ERR_INVALID, "GPU_NStream %d (context has %d streams)", nstream, ctx->nstream);
+  if (p->poisson && (!h_rho || !h_pot_in || !h_pot_out)) return fail(GPG_ERR_INVALID, "NULL host array");
+  if (p->gra_acc && (!h_flu || !h_pot_out)) return fail(GPG_ERR_INVALID, "NULL host array");
+  GPG_CUDA(cudaSetDevice(ctx->device));
+  ctx->last_npatch = npatch;
+  if (npatch == 0) return GPG_OK;
+
+  // per-stream chunks, CUAPI_Asyn_PoissonGravitySolver.cu:151-164
+  std::vector<int64_t> count(nstream), first(nstream);
+  first[0] = 0;
+  if (nstream == 1) {
+    count[0] = npatch;
+  } else {
+    for (int s = 0; s < nstream - 1; ++s) {
+      count[s] = npatch / nstream;
+      first[s + 1] = first[s] + count[s];
+    }
+    count[nstream - 1] = npatch - first[nstream - 1];
+  }
+  const size_t es = p->real_size;
+  auto bp = [](const void *base, int64_t off) { return (void *)((const char *)base + off); };
+  for (int s = 0; s < nstream; ++s) {
+    if (count[s] == 0) continue;
+    cudaStream_t st = ctx->streams[s];
+    const int64_t f = first[s], c = count[s];
+    if (p->poisson) {
+      GPG_CUDA(cudaMemcpyAsync(bp(ctx->d_rho, f * ctx->n_rho * es), bp(h_rho, f * ctx->n_rho * es),
+                               c * ctx->n_rho * es, cudaMemcpyHostToDevice, st));
+      GPG_CUDA(cudaMemcpyAsync(bp(ctx->d_pin, f * ctx->n_pin * es), bp(h_pot_in, f * ctx->n_pin * es),
+                               c * ctx->n_pin * es, cudaMemcpyHostToDevice, st));
+    }
+    if (p->gra_acc) {
+      if (!p->poisson)
+        GPG_CUDA(cudaMemcpyAsync(bp(ctx->d_pout, f * ctx->n_pout * es), bp(h_pot_out, f * ctx->n_pout * es),
+                                 c * ctx->n_pout * es, cudaMemcpyHostToDevice, st));
+      GPG_CUDA(cudaMemcpyAsync(bp(ctx->d_flu, f * ctx->n_flu * es), bp(h_flu, f * ctx->n_flu * es),
+                               c * ctx->n_flu * es, cudaMemcpyHostToDevice, st));
+    }
+  }
+  for (int s = 0; s < nstream; ++s) {
+    if (count[s] == 0) continue;
+    const int64_t f = first[s];
+    int rc = gpg_poisson_gravity_device(
+        p, (int)count[s], bp(ctx->d_rho, f * ctx->n_rho * es), bp(ctx->d_pin, f * ctx->n_pin * es),
+        bp(ctx->d_pout, f * ctx->n_pout * es), bp(ctx->d_flu, f * ctx->n_flu * es), nullptr,
+        p->poisson ? ctx->d_iters + f : nullptr, p->poisson ? ctx->d_resid + f : nullptr, ctx->streams[s]);
+    if (rc) return rc;
+  }
+  for (int s = 0; s < nstream; ++s) {
+    if (count[s] == 0) continue;
+    cudaStream_t st = ctx->streams[s];
+    const int64_t f = first[s], c = count[s];
+    if (p->poisson) {
+      GPG_CUDA(cudaMemcpyAsync(bp(h_pot_out, f * ctx->n_pout * es), bp(ctx->d_pout, f * ctx->n_pout * es),
+                               c * ctx->n_pout * es, cudaMemcpyDeviceToHost, st));
+      GPG_CUDA(cudaMemcpyAsync(ctx->h_iters + f, ctx->d_iters + f, c * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      GPG_CUDA(cudaMemcpyAsync(ctx->h_resid + f, ctx->d_resid + f, c * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    if (p->gra_acc)
+      GPG_CUDA(cudaMemcpyAsync(bp(h_flu, f * ctx->n_flu * es), bp(ctx->d_flu, f * ctx->n_flu * es),
+                               c * ctx->n_flu * es, cudaMemcpyDeviceToHost, st));
+  }
+  return GPG_OK;
+}
+
+extern "C" int gpg_synchronize(gpg_context *ctx) {
+  if (ctx) {
+    GPG_CUDA(cudaSetDevice(ctx->device));
+    for (auto s : ctx->streams) GPG_CUDA(cudaStreamSynchronize(s));
+  } else {
+    GPG_CUDA(cudaDeviceSynchronize());
+  }
+  GPG_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+extern "C" int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch) {
+  if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
+  if (npatch < 0 || npatch > ctx->last_npatch)
+    return fail(GPG_ERR_INVALID, "npatch %d (last solve had %lld)", npatch, (long long)ctx->last_npatch);
+  if (iters && npatch) std::memcpy(iters, ctx->h_iters, sizeof(int32_t) * npatch);
+  if (resid && npatch) std::memcpy(resid, ctx->h_resid, sizeof(double) * npatch);
+  return GPG_OK;
+}

@@ -26,6 +26,12 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#define GPG_API __attribute__((visibility("default")))
+#else
+#define GPG_API
+#endif
+
 #define GPG_NULL_INT 2147483647 /* NULL_INT, Header/Macro.h:73-75 */
 #define GPG_ABI_VERSION 1
 
@@ -87,17 +93,17 @@ typedef struct gpg_params {
  * omega / Min_Iter / Max_Iter of Main.cpp:1142-1157, MG settings of
  * Main.cpp:1173-1223, dt = 1e-2, dh = 1, Poi_Coeff = 4*pi*1e-5, CQUAD,
  * gra_ghost = 1, Poisson and GraAcc on. */
-int gpg_default_params(gpg_params *p, int real_size, int ghost, int scheme);
+GPG_API int gpg_default_params(gpg_params *p, int real_size, int ghost, int scheme);
 
 /* Check a parameter block (same checks as CUAPI_Asyn_PoissonGravitySolver.cu:116-140). */
-int gpg_validate_params(const gpg_params *p);
+GPG_API int gpg_validate_params(const gpg_params *p);
 
 /* Element counts per patch of each array for the shape in `p`. */
-int gpg_patch_sizes(const gpg_params *p, int64_t *rho, int64_t *pot_in, int64_t *pot_out,
+GPG_API int gpg_patch_sizes(const gpg_params *p, int64_t *rho, int64_t *pot_in, int64_t *pot_out,
                     int64_t *flu);
 
-const char *gpg_last_error(void);
-int gpg_abi_version(void);
+GPG_API const char *gpg_last_error(void);
+GPG_API int gpg_abi_version(void);
 
 /* ---------------------------------------------------------------------------
  * Stream-ordered device API.  All pointers are device pointers the caller owns;
@@ -110,7 +116,7 @@ int gpg_abi_version(void);
  * With poisson && gra_acc the gravity update is fused into the Poisson kernel
  * (one launch); with only gra_acc, d_pot_out is the input potential.
  * ------------------------------------------------------------------------- */
-int gpg_poisson_gravity_device(const gpg_params *p, int npatch, const void *d_rho,
+GPG_API int gpg_poisson_gravity_device(const gpg_params *p, int npatch, const void *d_rho,
                                const void *d_pot_in, void *d_pot_out, void *d_flu,
                                const void *d_guess, int32_t *d_iters, double *d_resid,
                                void *stream);
@@ -125,36 +131,36 @@ typedef struct gpg_context gpg_context;
 /* CUAPI_Set_Diagnose_Device (GPU_API/CUAPI_Set_Diagnose_Device.cu:45-292):
  * select the device and replace GPG_NULL_INT in *npgroup / *nstream with
  * defaults (streams: 4; patch groups: 32 * SM count). */
-int gpg_set_diagnose_device(int *npgroup, int *nstream, int device_id);
+GPG_API int gpg_set_diagnose_device(int *npgroup, int *nstream, int device_id);
 
-int gpg_context_create(gpg_context **ctx, int device_id, int nstream);
-int gpg_context_destroy(gpg_context *ctx);
+GPG_API int gpg_context_create(gpg_context **ctx, int device_id, int nstream);
+GPG_API int gpg_context_destroy(gpg_context *ctx);
 
 /* CUAPI_MemAllocate_PoissonGravity (GPU_API/CUAPI_MemAllocate_PoissonGravity.cu:27-80):
  * device buffers for npatch_group*8 patches of the shape in `shape`, plus pinned
  * host buffers returned through the four out-pointers. */
-int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int npatch_group,
+GPG_API int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int npatch_group,
                      void **h_rho, void **h_pot_in, void **h_pot_out, void **h_flu);
 
 /* CUAPI_MemFree_PoissonGravity (GPU_API/CUAPI_MemFree_PoissonGravity.cu:27-70). */
-int gpg_mem_free(gpg_context *ctx, void **h_rho, void **h_pot_in, void **h_pot_out,
+GPG_API int gpg_mem_free(gpg_context *ctx, void **h_rho, void **h_pot_in, void **h_pot_out,
                  void **h_flu);
 
 /* CUAPI_Asyn_PoissonGravitySolver (GPU_API/CUAPI_Asyn_PoissonGravitySolver.cu:85-275):
  * per stream, H2D of rho / pot_in (and pot_out when !poisson) / flu, the solve,
  * D2H of pot_out / flu.  Returns before the GPU finishes; call gpg_synchronize()
  * before reading h_pot_out / h_flu.  h_flu is in/out. */
-int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_rho, void *h_pot_in,
+GPG_API int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_rho, void *h_pot_in,
                                     void *h_pot_out, void *h_flu, int npatch_group,
                                     const gpg_params *p, int nstream);
 
 /* CUAPI_Synchronize (GPU_API/CUAPI_Synchronize.cu:10-13). */
-int gpg_synchronize(gpg_context *ctx);
+GPG_API int gpg_synchronize(gpg_context *ctx);
 
 /* Per-patch iteration counts / residuals of the last completed solve (host
  * copies; valid after gpg_synchronize).  No reference counterpart: the
  * reference only prints them (CPU_PoissonSolver_SOR.cpp:288). */
-int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
+GPG_API int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,75 @@
+"""C-ABI library checks that need no GPU: it loads, exports every symbol the
+header declares, and its host-side parameter logic matches the Python mirror."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from gpg.abi import GPG_MG, GPG_SOR, GpgParams, default_params
+from gpg.lib import GpgError, LIB_PATH, check, library
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = []
+    for h in os.listdir(os.path.join(REPO, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(REPO, "include", h)).read()
+            names += re.findall(r"^GPG_API\s+[^;(]*?\b(gpg_\w+)\s*\(", txt, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(LIB_PATH), "build with gpu_testbed_poisson-gravity_b200/build.py"
+    lib = C.CDLL(LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_params_struct_layout_matches_header():
+    # field offsets of struct gpg_params (include/gpg.h), naturally aligned
+    # (sizeof/offsetof as compiled by gcc from include/gpg.h)
+    assert C.sizeof(GpgParams) == 112
+    assert GpgParams.dt.offset == 32 and GpgParams.mg_tolerated_error.offset == 80
+    assert GpgParams.sor_tolerance.offset == 104
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+@pytest.mark.parametrize("g", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("scheme", [GPG_SOR, GPG_MG])
+def test_c_defaults_equal_python_defaults(rs, g, scheme):
+    p = GpgParams()
+    check(library().gpg_default_params(C.byref(p), rs, g, scheme))
+    assert p.as_dict() == default_params(rs, g, scheme).as_dict()
+    check(library().gpg_validate_params(C.byref(p)))
+
+
+@pytest.mark.parametrize("field,value", [("ghost", 0), ("ghost", 6), ("gra_ghost", 3), ("int_scheme", 1),
+                                         ("real_size", 2), ("scheme", 3), ("init_mode", 7),
+                                         ("stop_mode", 2), ("sor_max_iter", -1), ("p5_gradient", 1)])
+def test_validation_rejects(field, value):
+    p = default_params(4, 1, GPG_SOR).copy(**{field: value})
+    rc = library().gpg_validate_params(C.byref(p))
+    assert rc == 1
+    assert library().gpg_last_error()
+
+
+def test_patch_sizes():
+    p = default_params(4, 5, GPG_SOR, gra_ghost=2)
+    v = [C.c_int64() for _ in range(4)]
+    check(library().gpg_patch_sizes(C.byref(p), *[C.byref(x) for x in v]))
+    assert [x.value for x in v] == [16 ** 3, 12 ** 3, 12 ** 3, 2560]
+
+
+def test_device_call_without_gpu_reports_error():
+    """Without a CUDA device the library returns an error status, never a CPU result."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(GpgError):
+        from gpg.lib import set_diagnose_device
+        set_diagnose_device(0)

@@ -1,0 +1,180 @@
+"""CUDA library vs the CPU oracle, through the C-ABI (needs a B200).
+
+Tolerances (relative L-inf, max|gpu - ref| / max|ref| per patch):
+  * against the oracle with double residual sums (the library's arithmetic):
+      bit-identical fields wherever the iteration counts agree;
+  * against the reference CPU code (float residual sums):
+      1e-5 (FP32) / 1e-12 (FP64)  -- its stop decision may differ by a sweep
+      at the round-off floor.
+"""
+import numpy as np
+import pytest
+
+from gpg.abi import (GPG_INIT_GUESS, GPG_INIT_ZERO, GPG_INT_QUAD, GPG_MG, GPG_SOR,
+                     GPG_STOP_TOLERANCE, default_params)
+from gpg.inputs import make_patches
+from oracle.oracle import run_oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = {4: 1e-5, 8: 1e-12}
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gpg.lib import library
+    library()  # fails loudly when libgpg.so is missing
+    return torch
+
+
+def rel_linf(a, b):
+    a = np.asarray(a, dtype=np.float64).reshape(len(a), -1)
+    b = np.asarray(b, dtype=np.float64).reshape(len(b), -1)
+    return (np.abs(a - b).max(1) / np.abs(b).max(1)).max()
+
+
+def gpu_run(torch, p, d, guess=None):
+    from gpg.lib import solve_device
+    dev = torch.device("cuda:0")
+    t = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    flu = t(d["flu"]) if p.gra_acc else None
+    pot, flu, it, rs = solve_device(p, t(d["rho"]), t(d["pot_in"]), flu=flu, guess=t(guess))
+    torch.cuda.synchronize()
+    return (pot.cpu().numpy(), None if flu is None else flu.cpu().numpy(), it.cpu().numpy(),
+            rs.cpu().numpy())
+
+
+def compare(p, g_out, o_out):
+    """Fields bit-identical where sweeps agree; counts must agree for >= 99% of patches."""
+    gp, gf, gi, _ = g_out
+    op, of, oi, _ = o_out
+    same = gi == oi
+    assert same.mean() >= 0.99, f"iteration counts differ: {np.flatnonzero(~same)[:10]}"
+    assert np.array_equal(gp[same], op[same])
+    if gf is not None:
+        assert np.array_equal(gf[same], of[same])
+    if (~same).any():
+        assert rel_linf(gp[~same], op[~same]) <= TOL[p.real_size]
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+@pytest.mark.parametrize("g", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("scheme", [GPG_SOR, GPG_MG])
+def test_default_config_matches_oracle(torch_cuda, scheme, g, rs):
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(67, g, seed=300 + g, dtype=dt)   # odd count: partial CTA of teams
+    p = default_params(rs, g, scheme)
+    o = run_oracle(p, d["rho"], d["pot_in"], flu=d["flu"].copy(), accum_f64=True)
+    gout = gpu_run(torch_cuda, p, d)
+    compare(p, gout, o)
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+@pytest.mark.parametrize("g", [2, 3, 5])
+def test_p5_quad_variants(torch_cuda, g, rs):
+    dt = np.float32 if rs == 4 else np.float64
+    for scheme in (GPG_SOR, GPG_MG):
+        d = make_patches(16, g, seed=400 + g, gra_ghost=2, dtype=dt)
+        p = default_params(rs, g, scheme, gra_ghost=2, p5_gradient=1, int_scheme=GPG_INT_QUAD)
+        o = run_oracle(p, d["rho"], d["pot_in"], flu=d["flu"].copy(), accum_f64=True)
+        compare(p, gpu_run(torch_cuda, p, d), o)
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+@pytest.mark.parametrize("g", [1, 3, 5])
+def test_zero_start_tolerance_and_guess(torch_cuda, g, rs):
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(40, g, seed=500 + g, dtype=dt)
+    tol = 0.02 if rs == 4 else 5e-11
+    for mode in (GPG_INIT_ZERO, GPG_INIT_GUESS):
+        guess = None
+        if mode == GPG_INIT_GUESS:
+            rng = np.random.default_rng(g)
+            m = 6 + 2 * g
+            guess = (0.01 * rng.standard_normal((40, m, m, m))).astype(dt)
+        p = default_params(rs, g, GPG_SOR, init_mode=mode, stop_mode=GPG_STOP_TOLERANCE,
+                           sor_tolerance=tol, sor_min_iter=1, sor_max_iter=300)
+        o = run_oracle(p, d["rho"], d["pot_in"], flu=d["flu"].copy(), guess=guess, accum_f64=True)
+        compare(p, gpu_run(torch_cuda, p, d, guess=guess), o)
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+def test_gravity_alone(torch_cuda, rs):
+    dt = np.float32 if rs == 4 else np.float64
+    for G, p5 in ((1, 0), (2, 0), (2, 1)):
+        d = make_patches(24, 3, seed=600 + G, gra_ghost=G, dtype=dt)
+        gn = 8 + 2 * G
+        rng = np.random.default_rng(G)
+        pot = (0.01 * rng.standard_normal((24, gn, gn, gn))).astype(dt)
+        p = default_params(rs, 3, GPG_SOR, gra_ghost=G, p5_gradient=p5, poisson=0)
+        _, of, _, _ = run_oracle(p, None, None, pot_out=pot.copy(), flu=d["flu"].copy())
+        import torch
+        from gpg.lib import solve_device
+        tp = torch.from_numpy(pot).cuda()
+        tf = torch.from_numpy(d["flu"].copy()).cuda()
+        solve_device(p, None, None, pot_out=tp, flu=tf)
+        torch.cuda.synchronize()
+        assert np.array_equal(tf.cpu().numpy(), of)
+        assert np.array_equal(tp.cpu().numpy(), pot)  # read-only input
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+@pytest.mark.parametrize("scheme", [GPG_SOR, GPG_MG])
+def test_against_reference_golden(torch_cuda, scheme, rs):
+    """GPU vs outputs of the reference's own CPU code (tests/golden)."""
+    import json
+    import os
+    import sys
+    gold_dir = os.path.join(os.path.dirname(__file__), "golden")
+    sys.path.insert(0, gold_dir)
+    from make_golden import case_inputs
+    with open(os.path.join(gold_dir, "index.json")) as f:
+        idx = json.load(f)
+    n = 0
+    for name, c in idx["cases"].items():
+        if c["scheme"] != scheme or c["real_size"] != rs:
+            continue
+        d, _ = case_inputs(name, rs, c["ghost"], c["gra_ghost"])
+        gold = np.load(os.path.join(gold_dir, name + ".npz"))
+        p = default_params(rs, c["ghost"], scheme, gra_ghost=c["gra_ghost"],
+                           int_scheme=c["int_scheme"], p5_gradient=c["p5_gradient"])
+        gp, gf, gi, _ = gpu_run(torch_cuda, p, d)
+        keep = idx["keep_pot"]
+        assert rel_linf(gp[keep], gold["pot_out"]) <= TOL[rs], name
+        assert rel_linf(gf[:1], gold["flu"]) <= TOL[rs], name
+        if scheme == GPG_SOR:
+            assert (np.abs(gi - gold["iters"]) <= 2).all(), name
+        n += 1
+    assert n > 0
+
+
+def test_deterministic_and_batch_independent(torch_cuda):
+    """Same bits on repeat runs and whether a patch is solved alone or in a batch."""
+    for g in (1, 4):
+        d = make_patches(33, g, seed=700 + g, dtype=np.float32)
+        p = default_params(4, g, GPG_SOR)
+        a = gpu_run(torch_cuda, p, d)
+        b = gpu_run(torch_cuda, p, d)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+        single = {k: (v[5:6].copy() if k in ("rho", "pot_in", "flu") else v) for k, v in d.items()}
+        s = gpu_run(torch_cuda, p, single)
+        assert np.array_equal(s[0][0], a[0][5]) and s[2][0] == a[2][5]
+
+
+def test_empty_and_invalid(torch_cuda):
+    import torch
+    from gpg.lib import GpgError, solve_device
+    p = default_params(4, 2, GPG_SOR)
+    e = torch.empty((0, 10, 10, 10), device="cuda")
+    solve_device(p, e, torch.empty((0, 8, 8, 8), device="cuda"), flu=torch.empty((0, 5, 8, 8, 8), device="cuda"))
+    bad = default_params(4, 2, GPG_SOR, int_scheme=3)
+    d = make_patches(8, 2, seed=1)
+    with pytest.raises(GpgError) as ei:
+        gpu_run(torch, bad, d)
+    assert ei.value.status == 1
+    bad = default_params(4, 2, GPG_SOR, p5_gradient=1)  # needs gra_ghost 2
+    with pytest.raises(GpgError):
+        gpu_run(torch, bad, d)
