@@ -45,11 +45,14 @@ NPATCH = 4096
 L2_BYTES = 126 * 2 ** 20
 
 
-def workload(rank: int):
-    """[(params, inputs)] for the 8 batches of one step on this rank."""
+def workload(rank: int, only=None):
+    """[(params, inputs)] for the 8 batches of one step on this rank
+    (`only`: keep the batches named like f64_g5)."""
     out = []
     for rs in PRECS:
         for g in GHOSTS:
+            if only and f"f{8 * rs}_g{g}" not in only:
+                continue
             p = default_params(rs, g, GPG_SOR, gra_acc=0)
             dt = np.float32 if rs == 4 else np.float64
             d = make_patches(NPATCH, g, seed=1000 * (rank + 1) + g, dtype=dt, fluid=False)
@@ -170,6 +173,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", default=None,
+                    help="comma list of batches to run (e.g. f64_g5); profiling cases, not a bench line")
     a = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -211,7 +216,7 @@ def main(argv=None) -> int:
     from gpg.lib import Context, library, solve_device
     library()
 
-    batches = workload(rank)
+    batches = workload(rank, a.only.split(",") if a.only else None)
     dev_in = []
     for p, d in batches:
         n = len(d["rho"])
