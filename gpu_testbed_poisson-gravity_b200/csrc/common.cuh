@@ -41,31 +41,14 @@ struct Geo {
   static constexpr int U = G % 2;
   static constexpr int RHO3 = M * M * M;
   static constexpr int PN3 = PN * PN * PN;
-  // SOR team: one lane per x-pair of interior columns.
+  // number of interior x-pairs per patch (one SOR lane each)
   static constexpr int NPAIR = HALF * M;
-  static constexpr int TEAM = ((NPAIR + 31) / 32) * 32;
-  static constexpr int NWARP = TEAM / 32;
-  // Red/black-split cube in shared memory.  Plane (colour c, height z) holds
-  // N rows of HALF interior x-pairs (row pitch HALF, so the 32 lanes of a warp
-  // read 32 consecutive words) followed by the x = 0 and x = N-1 ghost cells
-  // of each row.
-  static constexpr int PP = N * HALF + 2 * N;
-  static constexpr int CUBE = 2 * N * PP;
 };
 
 // Colour of fine-cube cell (x, y, z): the SOR pass that updates it.  Pass 0 of
 // the reference (CPU_PoissonSolver_SOR.cpp:220-270) updates interior cells
 // whose rho index (x-1, y-1, z-1) has an even sum.
 __host__ __device__ constexpr int colour(int x, int y, int z) { return (x + y + z + 1) & 1; }
-
-template <int G>
-__device__ __forceinline__ int cube_addr(int x, int y, int z) {
-  using g = Geo<G>;
-  const int base = (colour(x, y, z) * g::N + z) * g::PP;
-  if (x == 0) return base + g::N * g::HALF + y;
-  if (x == g::N - 1) return base + g::N * g::HALF + g::N + y;
-  return base + y * g::HALF + ((x - 1) >> 1);
-}
 
 // Team barrier: a warp barrier for one-warp teams, a named barrier (id = team
 // index + 1, count = team threads) otherwise, so teams of one CTA that stop

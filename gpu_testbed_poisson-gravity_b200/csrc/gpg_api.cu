@@ -46,13 +46,25 @@ template <int G> constexpr int sor_ppc() { return G == 1 ? 4 : (G == 2 ? 2 : 1);
 // MG threads per CTA (one patch per CTA).
 template <int G> constexpr int mg_threads() { return G <= 2 ? 128 : 256; }
 
+// Kernel attributes, set once per kernel instantiation (the caller owns the
+// flag): the dynamic shared memory size and the max-shared carveout (the
+// reference's cudaFuncCachePreferShared, CUAPI_Set_Diagnose_Device.cu:274-285).
+struct AttrOnce {
+  std::once_flag once;
+  cudaError_t err = cudaSuccess;
+};
+
 template <typename KernelFn>
-int ensure_smem(KernelFn *fn, size_t bytes) {
-  if (bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess)
-      return fail(GPG_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(e));
-  }
+int ensure_smem(KernelFn *fn, size_t bytes, AttrOnce &st) {
+  std::call_once(st.once, [&] {
+    cudaError_t &err = st.err;
+    err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+  });
+  if (st.err != cudaSuccess)
+    return fail(GPG_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(st.err));
   return GPG_OK;
 }
 
@@ -62,9 +74,10 @@ int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   using S = gpg::SorSmem<T, G>;
   const size_t smem = PPC * S::team_bytes;
   auto fn = gpg::sor_kernel<T, G, PPC>;
-  if (int rc = ensure_smem(fn, smem)) return rc;
+  static AttrOnce attr;
+  if (int rc = ensure_smem(fn, smem, attr)) return rc;
   const int64_t grid = (a.npatch + PPC - 1) / PPC;
-  fn<<<(unsigned)grid, PPC * gpg::Geo<G>::TEAM, smem, s>>>(a);
+  fn<<<(unsigned)grid, PPC * gpg::SorCfg<T, G>::TEAM, smem, s>>>(a);
   GPG_CUDA(cudaGetLastError());
   return GPG_OK;
 }
@@ -74,7 +87,8 @@ int launch_mg(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   constexpr int NT = mg_threads<G>();
   const size_t smem = gpg::MgSmem<T, G, NT>::bytes;
   auto fn = gpg::mg_kernel<T, G, NT>;
-  if (int rc = ensure_smem(fn, smem)) return rc;
+  static AttrOnce attr;
+  if (int rc = ensure_smem(fn, smem, attr)) return rc;
   fn<<<(unsigned)a.npatch, NT, smem, s>>>(a);
   GPG_CUDA(cudaGetLastError());
   return GPG_OK;

@@ -51,9 +51,8 @@ struct MgSmem {
   using LV = MgLevels<G>;
   static constexpr size_t round(size_t b) { return (b + 15) / 16 * 16; }
   static constexpr size_t level_bytes = round(sizeof(T) * LV::total);
-  static constexpr size_t coarse_bytes = round(sizeof(T) * Geo<G>::PN3);
-  // sol, rhs, def for every level + coarse staging + reduction slots
-  static constexpr size_t bytes = 3 * level_bytes + coarse_bytes + round(2 * sizeof(double) * (NT / 32));
+  // sol, rhs, def for every level + reduction slots
+  static constexpr size_t bytes = 3 * level_bytes + round(2 * sizeof(double) * (NT / 32));
 };
 
 // Red-black Gauss-Seidel (CPU_PoissonSolver_MG.cpp:392-441): pass 0 updates
@@ -197,8 +196,7 @@ __global__ void __launch_bounds__(NT) mg_kernel(const SolveArgs<T> a) {
   T *s_sol = reinterpret_cast<T *>(smem_raw);
   T *s_rhs = reinterpret_cast<T *>(smem_raw + S::level_bytes);
   T *s_def = reinterpret_cast<T *>(smem_raw + 2 * S::level_bytes);
-  T *s_coarse = reinterpret_cast<T *>(smem_raw + 3 * S::level_bytes);
-  double *s_red = reinterpret_cast<double *>(smem_raw + 3 * S::level_bytes + S::coarse_bytes);
+  double *s_red = reinterpret_cast<double *>(smem_raw + 3 * S::level_bytes);
   const int tid = threadIdx.x;
   const int64_t P = blockIdx.x;
   if (P >= a.npatch) return;
@@ -213,13 +211,8 @@ __global__ void __launch_bounds__(NT) mg_kernel(const SolveArgs<T> a) {
   }
 
   // level-0 solution = interpolated cube; rhs0 = Poi_Coeff * rho; def boundaries 0
-  {
-    const T *src = a.pot_in + P * g::PN3;
-    for (int t = tid; t < g::PN3; t += NT) s_coarse[t] = src[t];
-    for (int t = tid; t < LV::total; t += NT) s_def[t] = T(0);
-  }
-  __syncthreads();
-  interpolate<T, G, NT>(s_coarse, tid, a.int_scheme,
+  for (int t = tid; t < LV::total; t += NT) s_def[t] = T(0);
+  interpolate<T, G, NT>(a.pot_in + P * g::PN3, tid, a.int_scheme,
                         [s_sol](int x, int y, int z, T v) { s_sol[(z * N + y) * N + x] = v; });
   {
     const T *rho = a.rho + P * g::RHO3;

@@ -11,17 +11,23 @@
 //      (or, in tolerance mode, once Total <= tol * sum|Const rho|); cap Max_Iter
 //   c. copy the GRA_NXT^3 window of the cube to pot_out
 //
-// B200 layout.  A team of TEAM = ceil(M*M/2 / 32)*32 threads owns a patch;
-// lane (y, h) owns the interior x-pair {2h+1, 2h+2} of row y at every height
-// and keeps both columns in registers, split by colour: v[c][z] is the lane's
-// colour-c cell at height z (one cell of each colour per pair and height).
-// A pass of colour p therefore updates v[p][z] for all heights and reads
+// B200 layout.  A team of 1-4 warps owns a patch.  Lane (y, h) owns the
+// interior x-pair {2h+1, 2h+2} of row y at every height and keeps both
+// columns in registers, split by colour: v[c][z] is the lane's colour-c cell
+// at height z (each pair has one cell of each colour per height).  A pass of
+// colour p updates v[p][z] for all heights and reads
 //   - z neighbours            v[1-p][z+-1]      (own registers)
 //   - one x neighbour         v[1-p][z]         (own registers, the pair mate)
 //   - other x and both y      shared memory     (3 loads)
-// and publishes the new value with one store.  The shared copy of the cube is
-// red/black split with a row pitch of HALF words, so a warp's 32 lanes touch
-// 32 consecutive words per access.  Two team barriers per sweep (one per
+// and publishes the new value with one store.
+//
+// Shared cube: plane (colour c, height z) has N rows of pitch P; slot s of a
+// row holds the colour-c cell among x = 2s-1, 2s (slot 0: x = 0 ghost, slot
+// H+1: x = N-1 ghost), so every x-neighbour read is own slot +-1.  Lanes are
+// grouped by row parity (odd rows first, R lanes per row), which makes the
+// read direction uniform inside a shared-memory wavefront; P is chosen per
+// (precision, ghost size) so that own, y+-1 and x-neighbour accesses of a
+// wavefront fall in distinct banks.  Two team barriers per sweep (one per
 // pass); the residual reduction rides on the second.
 #pragma once
 
@@ -33,67 +39,80 @@
 
 namespace gpg {
 
+// Lane mapping and row pitch per (precision, ghost size); see the file comment.
+template <typename T, int G>
+struct SorCfg {
+  using g = Geo<G>;
+  static constexpr bool F64 = sizeof(T) == 8;
+  // lanes per row (R >= HALF; R > HALF pads rows so wavefronts hold whole rows)
+  static constexpr int R = (G == 1) ? 4 : (G == 2 ? 5 : 8);
+  // row pitch (words), bank-conflict-free choice per configuration
+  static constexpr int P = (G == 1) ? (F64 ? 6 : 12) : (G == 2 ? (F64 ? 11 : 13) : (G == 3 ? (F64 ? 11 : 12) : 12));
+  static constexpr int ROWS_PER_CLASS = g::M / 2;
+  static constexpr int CW0 = ((ROWS_PER_CLASS * R + 15) / 16) * 16;
+  static constexpr int TEAM = ((2 * CW0 + 31) / 32) * 32;
+  static constexpr int CW = TEAM / 2;  // lanes per row-parity class
+  static constexpr int NWARP = TEAM / 32;
+  static constexpr int PP = g::N * P;  // plane pitch
+  static constexpr int CUBE = 2 * g::N * PP;
+  static_assert(R >= g::HALF && P >= g::HALF + 2, "row layout");
+
+  __device__ static __forceinline__ int addr(int x, int y, int z) {
+    return (colour(x, y, z) * g::N + z) * PP + y * P + ((x + 1) >> 1);
+  }
+};
+
 template <typename T, int G>
 struct SorSmem {
-  using g = Geo<G>;
-  // per team: cube + coarse staging + double-buffered warp partial sums
-  static constexpr int ALIGN = 16;
-  static constexpr size_t cube_bytes = sizeof(T) * g::CUBE;
-  static constexpr size_t coarse_bytes = sizeof(T) * g::PN3;
-  static constexpr size_t part_bytes = sizeof(double) * 2 * g::NWARP;
-  static constexpr size_t round(size_t b) { return (b + ALIGN - 1) / ALIGN * ALIGN; }
-  static constexpr size_t team_bytes = round(cube_bytes) + round(coarse_bytes) + round(part_bytes);
+  using C = SorCfg<T, G>;
+  static constexpr size_t round(size_t b) { return (b + 15) / 16 * 16; }
+  static constexpr size_t cube_bytes = sizeof(T) * C::CUBE;
+  static constexpr size_t part_bytes = sizeof(double) * 2 * C::NWARP;
+  static constexpr size_t team_bytes = round(cube_bytes) + round(part_bytes);
 };
 
 template <typename T, int G, int PPC>
-__global__ void __launch_bounds__(PPC *Geo<G>::TEAM)
+__global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
     sor_kernel(const SolveArgs<T> a) {
   using g = Geo<G>;
-  constexpr int N = g::N, M = g::M, HALF = g::HALF, TEAM = g::TEAM, NWARP = g::NWARP, PP = g::PP;
-  constexpr int PN3 = g::PN3, NPAIR = g::NPAIR;
+  using C = SorCfg<T, G>;
   using S = SorSmem<T, G>;
+  constexpr int N = g::N, M = g::M, HALF = g::HALF, TEAM = C::TEAM, NWARP = C::NWARP;
+  constexpr int P = C::P, PP = C::PP, R = C::R, CW = C::CW;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int team = threadIdx.x / TEAM, tid = threadIdx.x - team * TEAM;
   const int lane = tid & 31, warp = tid >> 5;
   unsigned char *tb = smem_raw + team * S::team_bytes;
   T *s_cube = reinterpret_cast<T *>(tb);
-  T *s_coarse = reinterpret_cast<T *>(tb + S::round(S::cube_bytes));
-  double *s_part = reinterpret_cast<double *>(tb + S::round(S::cube_bytes) + S::round(S::coarse_bytes));
+  double *s_part = reinterpret_cast<double *>(tb + S::round(S::cube_bytes));
 
-  const int64_t P = int64_t(blockIdx.x) * PPC + team;
-  if (P >= a.npatch) return;  // whole team leaves together
+  const int64_t P_ = int64_t(blockIdx.x) * PPC + team;
+  if (P_ >= a.npatch) return;  // whole team leaves together
 
-  // ---- stage the coarse potential and interpolate into the cube ----------
-  {
-    const T *src = a.pot_in + P * PN3;
-    for (int t = tid; t < PN3; t += TEAM) s_coarse[t] = src[t];
-  }
-  team_sync<TEAM>(team);
-  interpolate<T, G, TEAM>(s_coarse, tid, a.int_scheme,
-                          [s_cube](int x, int y, int z, T v) { s_cube[cube_addr<G>(x, y, z)] = v; });
+  // ---- interpolate the coarse potential into the cube (reads via L1) -----
+  interpolate<T, G, TEAM>(a.pot_in + P_ * g::PN3, tid, a.int_scheme,
+                          [s_cube](int x, int y, int z, T v) { s_cube[C::addr(x, y, z)] = v; });
   team_sync<TEAM>(team);
 
-  // ---- lane -> (y, h) pair, registers -------------------------------------
-  const bool active = tid < NPAIR;
-  const int q = active ? tid : 0;
-  const int y = 1 + q / HALF, h = q - (y - 1) * HALF;
-  const int own = y * HALF + h;  // in-plane offset of this lane's pair
-  // in-plane offset of the x neighbour outside the pair, for the cell on the
-  // left (x = 2h+1, neighbour x = 2h) and on the right (x = 2h+2, x = 2h+3)
-  const int xo_left = (h == 0) ? N * HALF + y : own - 1;
-  const int xo_right = (h == HALF - 1) ? N * HALF + N + y : own + 1;
-  // colour-c cell at height z sits on the left iff (y + z + c) is even
-  const int xo_even = (y & 1) ? xo_right : xo_left;  // used when (z + c) is even
-  const int xo_odd = (y & 1) ? xo_left : xo_right;   // used when (z + c) is odd
-  const bool left_even = !(y & 1);
+  // ---- lane -> (y, h): odd rows in lanes [0, CW), even rows in [CW, 2CW) --
+  const int cls = tid / CW, li = tid - cls * CW, r = li / R, h0 = li - r * R;
+  const bool active = (r < M / 2) && (h0 < HALF);
+  const int y = active ? 2 * r + 1 + cls : 1, h = active ? h0 : 0;
+  const int own = y * P + h + 1;  // in-plane offset of this lane's pair slot
+  // colour-c cell at height z sits on the left (x = 2h+1) iff (y + z + c) is
+  // even; its outside x neighbour is then slot own-1, else own+1.  With y's
+  // parity fixed per class the direction is uniform in a wavefront.
+  const bool left_even = !(y & 1);  // left when (z + c) is even
+  const int xo_even = left_even ? own - 1 : own + 1;
+  const int xo_odd = left_even ? own + 1 : own - 1;
 
   T v[2][N];
   T crho[2][M];
   double cr_sum = 0.0;
   {
-    const T *rho = a.rho + P * g::RHO3;
-    const T *guess = a.guess ? a.guess + P * g::RHO3 : nullptr;
+    const T *rho = a.rho + P_ * g::RHO3;
+    const T *guess = a.guess ? a.guess + P_ * g::RHO3 : nullptr;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
 #pragma unroll
@@ -103,23 +122,18 @@ __global__ void __launch_bounds__(PPC *Geo<G>::TEAM)
         const bool left = (((z + c) & 1) == 0) == left_even;
         const int x = left ? 2 * h + 1 : 2 * h + 2;
         const int idx = ((z - 1) * M + (y - 1)) * M + (x - 1);
-        crho[c][z - 1] = active ? mul(a.sor_const, rho[idx]) : T(0);
+        crho[c][z - 1] = active ? mul(a.sor_const, __ldg(rho + idx)) : T(0);
         cr_sum += (double)absval(crho[c][z - 1]);
-        if (a.init_mode != 0) {
-          const T init = (a.init_mode == 2 && active) ? guess[idx] : T(0);
-          v[c][z] = init;
-        }
+        if (a.init_mode != 0) v[c][z] = (a.init_mode == 2 && active) ? __ldg(guess + idx) : T(0);
       }
     }
   }
-  if (a.init_mode != 0) {
-    // the cube's interior must hold the new initial guess before any neighbour reads
-    if (active) {
+  if (a.init_mode != 0 && active) {
+    // publish the new interior guess before any neighbour read
 #pragma unroll
-      for (int c = 0; c < 2; ++c)
+    for (int c = 0; c < 2; ++c)
 #pragma unroll
-        for (int z = 1; z <= M; ++z) s_cube[(c * N + z) * PP + own] = v[c][z];
-    }
+      for (int z = 1; z <= M; ++z) s_cube[(c * N + z) * PP + own] = v[c][z];
   }
   double tol_abs = 0.0;
   if (a.stop_mode == 1) {
@@ -142,30 +156,38 @@ __global__ void __launch_bounds__(PPC *Geo<G>::TEAM)
   double total_old = (double)FLT_MAX, last = 0.0;
   int iter;
   for (iter = 0; iter < a.max_iter; ++iter) {
-    double acc = 0.0;
+    // four partial sums (heights z mod 4) keep the accumulation off the
+    // critical path; they are combined in a fixed order, so the total is
+    // deterministic and identical for a patch solved alone or in a batch
+    double acc4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
       if (active) {
         const T *nb = s_cube + (1 - p) * N * PP;  // planes of the other colour
         T *mine = s_cube + p * N * PP;
+        // all reads of the pass come from the other colour's planes and all
+        // writes go to this colour's planes: compute every height first and
+        // publish afterwards, so the updates of a pass overlap
 #pragma unroll
         for (int z = 1; z <= M; ++z) {
           const bool even = ((z + p) & 1) == 0;
           const bool left = even == left_even;
           const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
-          const T yp = nb[z * PP + own + HALF];
-          const T ym = nb[z * PP + own - HALF];
+          const T yp = nb[z * PP + own + P];
+          const T ym = nb[z * PP + own - P];
           const T mate = v[1 - p][z];
           const T xp = left ? mate : xo, xm = left ? xo : mate;
           const T s = add(add(add(add(add(v[1 - p][z + 1], v[1 - p][z - 1]), yp), ym), xp), xm);
-          const T r = sub(sub(s, mul(T(6), v[p][z])), crho[p][z - 1]);
-          v[p][z] = add(v[p][z], mul(omega_6, r));
-          mine[z * PP + own] = v[p][z];
-          acc += (double)absval(r);
+          const T res = sub(sub(s, mul(T(6), v[p][z])), crho[p][z - 1]);
+          v[p][z] = add(v[p][z], mul(omega_6, res));
+          acc4[z & 3] += (double)absval(res);
         }
+#pragma unroll
+        for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
       }
       if (p == 0) team_sync<TEAM>(team);
     }
+    double acc = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
     acc = warp_sum(acc);
     if constexpr (NWARP > 1) {
       if (lane == 0) s_part[(iter & 1) * NWARP + warp] = acc;
@@ -188,23 +210,23 @@ __global__ void __launch_bounds__(PPC *Geo<G>::TEAM)
     total_old = total;
   }
   if (tid == 0) {
-    if (a.iters) a.iters[P] = iter;
-    if (a.resid) a.resid[P] = last;
+    if (a.iters) a.iters[P_] = iter;
+    if (a.resid) a.resid[P_] = last;
   }
 
   // ---- output window (CPU_PoissonSolver_SOR.cpp:305-311) ------------------
   {
     const int GN = 8 + 2 * a.gra_ghost, shift = G - a.gra_ghost, GN3 = GN * GN * GN;
-    T *dst = a.pot_out + P * GN3;
+    T *dst = a.pot_out + P_ * GN3;
     for (int t = tid; t < GN3; t += TEAM) {
       const int i = t % GN, j = (t / GN) % GN, k = t / (GN * GN);
-      dst[t] = s_cube[cube_addr<G>(i + shift, j + shift, k + shift)];
+      dst[t] = s_cube[C::addr(i + shift, j + shift, k + shift)];
     }
   }
   // ---- fused gravity update (CPU_GravitySolver.cpp:34-79) -----------------
   if (a.gra_acc) {
-    gravity_patch<T, TEAM>(a.flu + P * 5 * 512, tid, a.gra_const, a.p5,
-                           [s_cube](int i, int j, int k) { return s_cube[cube_addr<G>(i + G, j + G, k + G)]; });
+    gravity_patch<T, TEAM>(a.flu + P_ * 5 * 512, tid, a.gra_const, a.p5,
+                           [s_cube](int i, int j, int k) { return s_cube[C::addr(i + G, j + G, k + G)]; });
   }
 }
 
