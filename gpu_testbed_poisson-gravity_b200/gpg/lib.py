@@ -158,7 +158,7 @@ class Context:
         """CUAPI_Asyn_PoissonGravitySolver on the allocated pinned buffers (or
         on `host` = (rho, pot_in, pot_out, flu) numpy arrays)."""
         if host is None:
-            ptrs = self._host
+            ptrs = self._host if self._host is not None else [None] * 4
         else:
             ptrs = [C.c_void_p(a.ctypes.data) if a is not None else None for a in host]
         check(library().gpg_asyn_poisson_gravity_solver(self._ctx, ptrs[0], ptrs[1], ptrs[2], ptrs[3],

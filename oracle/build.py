@@ -98,6 +98,57 @@ def _build_one(ref_root: str, scheme: str, g: int, G: int, prec: str) -> str:
     return out
 
 
+# ---------------------------------------------------------------------------
+# integration: the reference's own driver (Main.cpp) relinked on libgpg
+# ---------------------------------------------------------------------------
+PKG = os.path.join(REPO, "gpu_testbed_poisson-gravity_b200")
+SHIM = os.path.join(PKG, "csrc", "cuapi", "cuapi_compat.cpp")
+LIBGPG_DIR = os.path.join(PKG, "lib")
+# (scheme, POT_GHOST_SIZE, GRA_GHOST_SIZE, precision)
+INTEGRATION_CONFIGS = [("sor", 1, 1, "f32"), ("sor", 5, 1, "f32"), ("sor", 3, 2, "f64"),
+                       ("mg", 3, 2, "f32"), ("mg", 2, 1, "f64")]
+# DataCompare thresholds of the reference Makefile (Makefile:56-70)
+MAXERR = {("sor", "f32"): ("5.e-6", "8.e-6"), ("sor", "f64"): ("3.e-15", "1.e-14"),
+          ("mg", "f32"): ("4.e-5", "4.e-5"), ("mg", "f64"): ("3.e-14", "3.e-14")}
+
+
+def integration_exe(scheme, g, G, prec):
+    return os.path.join(REF_OUT, f"main_{scheme}_g{g}_G{G}_{prec}")
+
+
+def _build_integration_one(ref_root, scheme, g, G, prec):
+    out = integration_exe(scheme, g, G, prec)
+    srcs = [os.path.join(ref_root, "Main.cpp")] + [os.path.join(ref_root, s) for s in REF_SOURCES]
+    deps = srcs + [SHIM, os.path.join(REPO, "include", "gpg_cuapi.h"), os.path.join(LIBGPG_DIR, "libgpg.so")]
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+        return out
+    poi, gra = MAXERR[(scheme, prec)]
+    macros = reference_macros(scheme, g, G, prec) + [
+        "-DCPULOAD=420000", "-DINIT_WIDTH=410.0", "-DINIT_INDEX=2.1", "-DINIT_OFFSET=0.09",
+        f"-DPOI_MAXERR={poi}", f"-DGRA_MAXERR={gra}"]
+    shim_macros = [m for m in macros if not m.startswith("-DPOT_SCHEME")] + [
+        f"-DPOT_SCHEME={1 if scheme == 'sor' else 2}"]
+    shim_obj = out + "_shim.o"
+    _run(["g++", "-O2", "-fPIC", "-c", "-o", shim_obj, SHIM] + shim_macros)
+    _run(["g++", "-O3", "-fopenmp", "-w", "-I" + os.path.join(ref_root, "Header")] + macros
+         + ["-o", out] + srcs + [shim_obj, "-L" + LIBGPG_DIR, "-lgpg",
+                                 "-Wl,-rpath,$ORIGIN/../../gpu_testbed_poisson-gravity_b200/lib"])
+    return out
+
+
+def build_integration(ref_root: str = DEFAULT_REF) -> list[str]:
+    """Link the reference's unmodified Main.cpp + CPU solvers against the CUAPI
+    shim and libgpg (one executable per configuration, in oracle/_ref/)."""
+    if not os.path.isdir(os.path.join(ref_root, "CPU_Solver")):
+        return []
+    if not os.path.exists(os.path.join(LIBGPG_DIR, "libgpg.so")):
+        raise RuntimeError("build libgpg.so first")
+    os.makedirs(REF_OUT, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        futs = [ex.submit(_build_integration_one, ref_root, *c) for c in INTEGRATION_CONFIGS]
+        return [f.result() for f in futs]
+
+
 def build_ref(ref_root: str = DEFAULT_REF, jobs: int | None = None) -> list[str]:
     """Compile every reference configuration; returns the built paths.
     Does nothing (returns []) when the reference tree is absent."""
@@ -119,6 +170,8 @@ def main(argv=None) -> int:
     if not a.no_ref:
         libs = build_ref(a.ref)
         print(f"{len(libs)} reference configurations in {REF_OUT}")
+        exes = build_integration(a.ref)
+        print(f"{len(exes)} integration executables in {REF_OUT}")
     return 0
 
 
