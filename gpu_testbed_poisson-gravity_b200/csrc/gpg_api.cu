@@ -2,10 +2,12 @@
 // dispatch, and the reference-shaped context API (device buffers, pinned host
 // buffers, streams) that replaces GPU_API/CUAPI_*.cu.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -41,8 +43,6 @@ int fail(int status, const char *fmt, ...) {
 // ---------------------------------------------------------------------------
 // launch configuration per (precision, ghost size)
 // ---------------------------------------------------------------------------
-// SOR teams per CTA: aim for 128-thread CTAs (teams of 32/64/96/128/128 threads).
-template <int G> constexpr int sor_ppc() { return G == 1 ? 4 : (G == 2 ? 2 : 1); }
 // MG threads per CTA (one patch per CTA).
 template <int G> constexpr int mg_threads() { return G <= 2 ? 128 : 256; }
 
@@ -52,6 +52,7 @@ template <int G> constexpr int mg_threads() { return G <= 2 ? 128 : 256; }
 struct AttrOnce {
   std::once_flag once;
   cudaError_t err = cudaSuccess;
+  int max_threads = 0;  // per block, given the kernel's registers
 };
 
 template <typename KernelFn>
@@ -62,24 +63,82 @@ int ensure_smem(KernelFn *fn, size_t bytes, AttrOnce &st) {
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncAttributes fa;
+    if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, fn);
+    if (err == cudaSuccess) st.max_threads = fa.maxThreadsPerBlock;
   });
   if (st.err != cudaSuccess)
     return fail(GPG_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(st.err));
   return GPG_OK;
 }
 
-template <typename T, int G>
-int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
-  constexpr int PPC = sor_ppc<G>();
+// SOR kernel variants: (teams per CTA, phased pass).  The table below holds
+// the variant per (precision, ghost size); defaults are the fastest measured
+// on B200, gpg_set_sor_variant / a tuning file override them.
+constexpr int kSorVariants = 6;
+constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4};
+constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true};
+int g_sor_variant[2][6] = {
+    // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
+    {0, 1, 1, 1, 0, 1},   // float
+    {0, 4, 2, 0, 0, 1},   // double
+};
+std::once_flag g_tune_once;
+
+void load_tune_file() {
+  // optional text file, one "f32|f64 <ghost> <variant>" per line:
+  // $GPG_TUNE_FILE, else sor_tune.txt beside libgpg.so (written by autotune.py)
+  const char *path = std::getenv("GPG_TUNE_FILE");
+  std::string p;
+  if (path) {
+    p = path;
+  } else {
+    Dl_info info;
+    if (dladdr((void *)&load_tune_file, &info) && info.dli_fname) {
+      p = info.dli_fname;
+      p = p.substr(0, p.find_last_of('/') + 1) + "sor_tune.txt";
+    }
+  }
+  if (p.empty()) return;
+  FILE *f = std::fopen(p.c_str(), "r");
+  if (!f) return;
+  char prec[8];
+  int g, v;
+  while (std::fscanf(f, "%7s %d %d", prec, &g, &v) == 3) {
+    const int t = std::strcmp(prec, "f64") == 0 ? 1 : (std::strcmp(prec, "f32") == 0 ? 0 : -1);
+    if (t >= 0 && g >= 1 && g <= 5 && v >= 0 && v < kSorVariants) g_sor_variant[t][g] = v;
+  }
+  std::fclose(f);
+}
+
+template <typename T, int G, int PPC, bool PHASED>
+int launch_sor_v(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   using S = gpg::SorSmem<T, G>;
   const size_t smem = PPC * S::team_bytes;
-  auto fn = gpg::sor_kernel<T, G, PPC>;
+  if (smem > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %zu bytes of shared memory", smem);
+  auto fn = gpg::sor_kernel<T, G, PPC, PHASED>;
   static AttrOnce attr;
   if (int rc = ensure_smem(fn, smem, attr)) return rc;
+  if (PPC * gpg::SorCfg<T, G>::TEAM > attr.max_threads)
+    return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %d threads per CTA (registers allow %d)",
+                PPC * gpg::SorCfg<T, G>::TEAM, attr.max_threads);
   const int64_t grid = (a.npatch + PPC - 1) / PPC;
   fn<<<(unsigned)grid, PPC * gpg::SorCfg<T, G>::TEAM, smem, s>>>(a);
   GPG_CUDA(cudaGetLastError());
   return GPG_OK;
+}
+
+template <typename T, int G>
+int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  std::call_once(g_tune_once, load_tune_file);
+  switch (g_sor_variant[sizeof(T) == 8][G]) {
+    case 0: return launch_sor_v<T, G, 1, false>(a, s);
+    case 1: return launch_sor_v<T, G, 1, true>(a, s);
+    case 2: return launch_sor_v<T, G, 2, false>(a, s);
+    case 3: return launch_sor_v<T, G, 2, true>(a, s);
+    case 4: return launch_sor_v<T, G, 4, false>(a, s);
+    default: return launch_sor_v<T, G, 4, true>(a, s);
+  }
 }
 
 template <typename T, int G>
@@ -531,5 +590,33 @@ extern "C" int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *res
     return fail(GPG_ERR_INVALID, "npatch %d (last solve had %lld)", npatch, (long long)ctx->last_npatch);
   if (iters && npatch) std::memcpy(iters, ctx->h_iters, sizeof(int32_t) * npatch);
   if (resid && npatch) std::memcpy(resid, ctx->h_resid, sizeof(double) * npatch);
+  return GPG_OK;
+}
+
+// ===========================================================================
+// SOR kernel variants (autotuning)
+// ===========================================================================
+extern "C" int gpg_sor_variant_count(void) { return kSorVariants; }
+
+extern "C" int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased) {
+  if (variant < 0 || variant >= kSorVariants) return fail(GPG_ERR_INVALID, "variant %d", variant);
+  if (patches_per_cta) *patches_per_cta = kSorVariantPPC[variant];
+  if (phased) *phased = kSorVariantPhased[variant];
+  return GPG_OK;
+}
+
+extern "C" int gpg_set_sor_variant(int real_size, int ghost, int variant) {
+  std::call_once(g_tune_once, load_tune_file);
+  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < 0 || variant >= kSorVariants)
+    return fail(GPG_ERR_INVALID, "real_size %d ghost %d variant %d", real_size, ghost, variant);
+  g_sor_variant[real_size == 8][ghost] = variant;
+  return GPG_OK;
+}
+
+extern "C" int gpg_get_sor_variant(int real_size, int ghost, int *variant) {
+  std::call_once(g_tune_once, load_tune_file);
+  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || !variant)
+    return fail(GPG_ERR_INVALID, "real_size %d ghost %d", real_size, ghost);
+  *variant = g_sor_variant[real_size == 8][ghost];
   return GPG_OK;
 }

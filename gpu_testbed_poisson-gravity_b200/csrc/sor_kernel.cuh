@@ -71,7 +71,71 @@ struct SorSmem {
   static constexpr size_t team_bytes = round(cube_bytes) + round(part_bytes);
 };
 
-template <typename T, int G, int PPC>
+// One pass of colour p over every height of the lane's pair: reads the other
+// colour (registers + 3 shared loads per cell), updates v[p][*] in registers,
+// then publishes them.  SUM: accumulate |R| into acc4 (skipped for sweeps
+// whose residual total the stopping rule never looks at).
+template <typename T, int G, bool PHASED, int p, bool SUM>
+__device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2][Geo<G>::M], T *s_cube,
+                                         int own, int xo_even, int xo_odd, bool left_even, T omega_6,
+                                         double (&acc4)[4]) {
+  using C = SorCfg<T, G>;
+  constexpr int N = Geo<G>::N, M = Geo<G>::M, P = C::P, PP = C::PP;
+  const T *nb = s_cube + (1 - p) * N * PP;  // planes of the other colour
+  T *mine = s_cube + p * N * PP;
+  // all reads of the pass come from the other colour's planes and all writes
+  // go to this colour's planes, so the M updates are independent; the stores
+  // follow all of them
+  if constexpr (PHASED) {
+    // phase by phase across all heights, keeping the reference's operand
+    // order within each cell
+    T sum[M];
+#pragma unroll
+    for (int z = 1; z <= M; ++z) sum[z - 1] = add(v[1 - p][z + 1], v[1 - p][z - 1]);
+#pragma unroll
+    for (int z = 1; z <= M; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own + P]);
+#pragma unroll
+    for (int z = 1; z <= M; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own - P]);
+#pragma unroll
+    for (int z = 1; z <= M; ++z) {
+      const bool even = ((z + p) & 1) == 0;
+      const bool left = even == left_even;
+      const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
+      const T mate = v[1 - p][z];
+      const T xp = left ? mate : xo, xm = left ? xo : mate;
+      sum[z - 1] = add(add(sum[z - 1], xp), xm);
+    }
+#pragma unroll
+    for (int z = 1; z <= M; ++z) {
+      const T res = sub(sub(sum[z - 1], mul(T(6), v[p][z])), crho[p][z - 1]);
+      v[p][z] = add(v[p][z], mul(omega_6, res));
+      if constexpr (SUM) acc4[z & 3] += (double)absval(res);
+    }
+  } else {
+#pragma unroll
+    for (int z = 1; z <= M; ++z) {
+      const bool even = ((z + p) & 1) == 0;
+      const bool left = even == left_even;
+      const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
+      const T yp = nb[z * PP + own + P];
+      const T ym = nb[z * PP + own - P];
+      const T mate = v[1 - p][z];
+      const T xp = left ? mate : xo, xm = left ? xo : mate;
+      const T sm = add(add(add(add(add(v[1 - p][z + 1], v[1 - p][z - 1]), yp), ym), xp), xm);
+      const T res = sub(sub(sm, mul(T(6), v[p][z])), crho[p][z - 1]);
+      v[p][z] = add(v[p][z], mul(omega_6, res));
+      if constexpr (SUM) acc4[z & 3] += (double)absval(res);
+    }
+  }
+#pragma unroll
+  for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
+}
+
+// PPC: teams (patches) per CTA.  PHASED: form the M independent updates of a
+// pass phase by phase across heights (more updates in flight, more registers)
+// instead of height by height.  Both orders give identical bits; the
+// autotuner (gpg_set_sor_variant) picks per (precision, ghost size).
+template <typename T, int G, int PPC, bool PHASED>
 __global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
     sor_kernel(const SolveArgs<T> a) {
   using g = Geo<G>;
@@ -156,37 +220,24 @@ __global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
   double total_old = (double)FLT_MAX, last = 0.0;
   int iter;
   for (iter = 0; iter < a.max_iter; ++iter) {
+    // The stopping rule reads the residual total from sweep Min_Iter-2 on
+    // (the growth test compares with the previous sweep) and the final
+    // report needs the last sweep's; earlier sweeps skip the sums.
+    const bool need = (iter + 2 >= a.min_iter) || (iter + 1 == a.max_iter);
     // four partial sums (heights z mod 4) keep the accumulation off the
     // critical path; they are combined in a fixed order, so the total is
     // deterministic and identical for a patch solved alone or in a batch
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      if (active) {
-        const T *nb = s_cube + (1 - p) * N * PP;  // planes of the other colour
-        T *mine = s_cube + p * N * PP;
-        // all reads of the pass come from the other colour's planes and all
-        // writes go to this colour's planes: compute every height first and
-        // publish afterwards, so the updates of a pass overlap
-#pragma unroll
-        for (int z = 1; z <= M; ++z) {
-          const bool even = ((z + p) & 1) == 0;
-          const bool left = even == left_even;
-          const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
-          const T yp = nb[z * PP + own + P];
-          const T ym = nb[z * PP + own - P];
-          const T mate = v[1 - p][z];
-          const T xp = left ? mate : xo, xm = left ? xo : mate;
-          const T s = add(add(add(add(add(v[1 - p][z + 1], v[1 - p][z - 1]), yp), ym), xp), xm);
-          const T res = sub(sub(s, mul(T(6), v[p][z])), crho[p][z - 1]);
-          v[p][z] = add(v[p][z], mul(omega_6, res));
-          acc4[z & 3] += (double)absval(res);
-        }
-#pragma unroll
-        for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
-      }
-      if (p == 0) team_sync<TEAM>(team);
+    if (!need) {
+      if (active) sor_pass<T, G, PHASED, 0, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      team_sync<TEAM>(team);
+      if (active) sor_pass<T, G, PHASED, 1, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      team_sync<TEAM>(team);
+      continue;
     }
+    if (active) sor_pass<T, G, PHASED, 0, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    team_sync<TEAM>(team);
+    if (active) sor_pass<T, G, PHASED, 1, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
     double acc = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
     acc = warp_sum(acc);
     if constexpr (NWARP > 1) {

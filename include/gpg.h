@@ -162,6 +162,19 @@ GPG_API int gpg_synchronize(gpg_context *ctx);
  * reference only prints them (CPU_PoissonSolver_SOR.cpp:288). */
 GPG_API int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
 
+/* ---------------------------------------------------------------------------
+ * SOR kernel variants.  No reference counterpart (the reference fixes its
+ * launch shape per ghost size with macros, Header/CUPOT.h:44-90).  A variant
+ * is (patches per CTA, phased pass order); results are bit-identical across
+ * variants.  The table starts from the library's defaults, then an optional
+ * tuning file ($GPG_TUNE_FILE, else sor_tune.txt beside libgpg.so, lines
+ * "f32|f64 <ghost> <variant>") written by autotune.py.
+ * ------------------------------------------------------------------------- */
+GPG_API int gpg_sor_variant_count(void);
+GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased);
+GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
+GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,43 @@
+"""Every SOR kernel variant (patches per CTA x pass order) returns the same
+bits as every other (needs a B200)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpg.abi import GPG_SOR, default_params
+from gpg.inputs import make_patches
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("rs,g", [(4, 1), (4, 3), (8, 2), (8, 5)])
+def test_variants_bit_identical(rs, g):
+    torch = pytest.importorskip("torch")
+    from gpg.lib import GpgError, check, library, solve_device
+    lib = library()
+    dev = torch.device("cuda:0")
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(37, g, seed=900 + g, dtype=dt)
+    p = default_params(rs, g, GPG_SOR)
+    cur = C.c_int()
+    check(lib.gpg_get_sor_variant(rs, g, C.byref(cur)))
+    outs = []
+    try:
+        for v in range(lib.gpg_sor_variant_count()):
+            check(lib.gpg_set_sor_variant(rs, g, v))
+            try:
+                pot, flu, it, rsd = solve_device(p, torch.from_numpy(d["rho"]).to(dev),
+                                                 torch.from_numpy(d["pot_in"]).to(dev),
+                                                 flu=torch.from_numpy(d["flu"].copy()).to(dev))
+            except GpgError as e:
+                assert e.status == 5  # variant does not fit (shared memory / registers)
+                continue
+            torch.cuda.synchronize()
+            outs.append((v, pot.cpu().numpy(), flu.cpu().numpy(), it.cpu().numpy(), rsd.cpu().numpy()))
+    finally:
+        check(lib.gpg_set_sor_variant(rs, g, cur.value))
+    assert len(outs) >= 2
+    for v, *o in outs[1:]:
+        for a, b in zip(o, outs[0][1:]):
+            assert np.array_equal(a, b), f"variant {v}"
