@@ -9,11 +9,14 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
 #include "../../include/gpg.h"
+#include "batch_kernel.cuh"
 #include "gravity.cuh"
 #include "mg_kernel.cuh"
 #include "sor_kernel.cuh"
@@ -295,8 +298,8 @@ extern "C" int gpg_validate_params(const gpg_params *p) {
     if (p->scheme == GPG_SOR) {
       if (p->sor_max_iter < 0) return fail(GPG_ERR_INVALID, "sor_max_iter %d", p->sor_max_iter);
       if (p->init_mode < 0 || p->init_mode > 2) return fail(GPG_ERR_INVALID, "init_mode %d", p->init_mode);
-      if (p->stop_mode < 0 || p->stop_mode > 1) return fail(GPG_ERR_INVALID, "stop_mode %d", p->stop_mode);
-      if (p->stop_mode == GPG_STOP_TOLERANCE && !(p->sor_tolerance >= 0.0))
+      if (p->stop_mode < 0 || p->stop_mode > 2) return fail(GPG_ERR_INVALID, "stop_mode %d", p->stop_mode);
+      if (p->stop_mode != GPG_STOP_REFERENCE && !(p->sor_tolerance >= 0.0))
         return fail(GPG_ERR_INVALID, "sor_tolerance %g", p->sor_tolerance);
     } else {
       if (p->mg_max_iter < 0 || p->mg_npre_smooth < 0 || p->mg_npost_smooth < 0)
@@ -618,5 +621,171 @@ extern "C" int gpg_get_sor_variant(int real_size, int ghost, int *variant) {
   if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || !variant)
     return fail(GPG_ERR_INVALID, "real_size %d ghost %d", real_size, ghost);
   *variant = g_sor_variant[real_size == 8][ghost];
+  return GPG_OK;
+}
+
+// ===========================================================================
+// batched mixed-ghost-size SOR (persistent kernel + device work queue)
+// ===========================================================================
+namespace {
+
+const double kDefaultOmega[5] = {1.49, 1.57, 1.62, 1.65, 1.69};  // Main.cpp:1145
+
+template <typename T>
+struct BatchLaunchCfg {
+  AttrOnce attr;
+  std::once_flag occ_once;
+  int blocks_per_sm = 0;
+  int sms = 0;
+  cudaError_t err = cudaSuccess;
+};
+
+template <typename T>
+int batch_prepare(BatchLaunchCfg<T> *&out) {
+  static BatchLaunchCfg<T> cfg;
+  const size_t smem = gpg::batch_smem_bytes<T>();
+  if (int rc = ensure_smem(gpg::sor_batch_kernel<T>, smem, cfg.attr)) return rc;
+  std::call_once(cfg.occ_once, [&] {
+    int dev = 0;
+    cfg.err = cudaGetDevice(&dev);
+    if (cfg.err == cudaSuccess) cfg.err = cudaDeviceGetAttribute(&cfg.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cfg.err == cudaSuccess)
+      cfg.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, gpg::sor_batch_kernel<T>,
+                                                              gpg::kBatchThreads, smem);
+  });
+  if (cfg.err != cudaSuccess) return fail(GPG_ERR_CUDA, "batch occupancy: %s", cudaGetErrorString(cfg.err));
+  if (cfg.blocks_per_sm < 1) return fail(GPG_ERR_UNSUPPORTED, "batch kernel does not fit on an SM");
+  out = &cfg;
+  return GPG_OK;
+}
+
+int validate_batch(const gpg_params *p, int ngroup, const gpg_batch_group *groups) {
+  if (int rc = gpg_validate_params(p)) return rc;
+  if (!p->poisson || p->scheme != GPG_SOR) return fail(GPG_ERR_UNSUPPORTED, "batched solve is SOR only");
+  if (ngroup < 0 || ngroup > GPG_BATCH_MAX_GROUPS)
+    return fail(GPG_ERR_INVALID, "ngroup %d (max %d)", ngroup, GPG_BATCH_MAX_GROUPS);
+  if (ngroup && !groups) return fail(GPG_ERR_INVALID, "groups is NULL");
+  for (int i = 0; i < ngroup; ++i) {
+    const gpg_batch_group &g = groups[i];
+    gpg_params q = *p;
+    q.ghost = g.ghost;
+    if (int rc = gpg_validate_params(&q)) return rc;
+    if (g.npatch < 0) return fail(GPG_ERR_INVALID, "group %d: npatch %d", i, g.npatch);
+    if (g.npatch == 0) continue;
+    if (!g.d_rho || !g.d_pot_in || !g.d_pot_out) return fail(GPG_ERR_INVALID, "group %d: NULL array", i);
+    if (p->gra_acc && !g.d_flu) return fail(GPG_ERR_INVALID, "group %d: d_flu is NULL", i);
+    if (p->init_mode == GPG_INIT_GUESS && !g.d_guess) return fail(GPG_ERR_INVALID, "group %d: d_guess is NULL", i);
+  }
+  return GPG_OK;
+}
+
+template <typename T>
+int solve_batch_typed(const gpg_params &p, int ngroup, const gpg_batch_group *groups, uint32_t *counter,
+                      cudaStream_t s) {
+  gpg::BatchArgs<T> b{};
+  std::vector<int> order(ngroup);
+  std::iota(order.begin(), order.end(), 0);
+  // largest cubes first: their units are the longest, so they start earliest
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return groups[x].ghost > groups[y].ghost; });
+  int64_t u = 0;
+  int k = 0;
+  for (int idx : order) {
+    const gpg_batch_group &gr = groups[idx];
+    if (gr.npatch == 0) continue;
+    gpg_params q = p;
+    q.ghost = gr.ghost;
+    q.sor_omega = gr.sor_omega > 0 ? gr.sor_omega : kDefaultOmega[gr.ghost - 1];
+    b.grp[k] = make_args<T>(q, gr.npatch, gr.d_rho, gr.d_pot_in, gr.d_pot_out, gr.d_flu, gr.d_guess, gr.d_iters,
+                            gr.d_resid);
+    b.ghost[k] = gr.ghost;
+    b.unit_start[k] = u;
+    const int ppu = gpg::batch_patches_per_unit<T>(gr.ghost);
+    u += (gr.npatch + ppu - 1) / ppu;
+    ++k;
+  }
+  b.unit_start[k] = u;
+  b.ngroup = k;
+  b.nunit = u;
+  b.counter = counter;
+  if (u == 0) return GPG_OK;
+  BatchLaunchCfg<T> *cfg = nullptr;
+  if (int rc = batch_prepare<T>(cfg)) return rc;
+  const int64_t grid = std::min<int64_t>(u, (int64_t)cfg->sms * cfg->blocks_per_sm);
+  GPG_CUDA(cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
+  gpg::sor_batch_kernel<T><<<(unsigned)grid, gpg::kBatchThreads, gpg::batch_smem_bytes<T>(), s>>>(b);
+  GPG_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+}  // namespace
+
+extern "C" int gpg_solve_batch_device(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
+                                      uint32_t *d_counter, void *stream) {
+  if (int rc = validate_batch(p, ngroup, groups)) return rc;
+  if (!d_counter) return fail(GPG_ERR_INVALID, "d_counter is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return p->real_size == 4 ? solve_batch_typed<float>(*p, ngroup, groups, d_counter, s)
+                           : solve_batch_typed<double>(*p, ngroup, groups, d_counter, s);
+}
+
+struct gpg_batch_plan {
+  int device = 0;
+  uint32_t *d_counter = nullptr;
+  cudaStream_t capture = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int gpg_batch_plan_destroy(gpg_batch_plan *plan) {
+  if (!plan) return GPG_OK;
+  cudaSetDevice(plan->device);
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->graph) cudaGraphDestroy(plan->graph);
+  if (plan->capture) cudaStreamDestroy(plan->capture);
+  if (plan->d_counter) cudaFree(plan->d_counter);
+  delete plan;
+  return GPG_OK;
+}
+
+extern "C" int gpg_batch_plan_create(gpg_batch_plan **out, const gpg_params *p, int ngroup,
+                                     const gpg_batch_group *groups, int device_id) {
+  if (!out) return fail(GPG_ERR_INVALID, "plan is NULL");
+  *out = nullptr;
+  if (int rc = validate_batch(p, ngroup, groups)) return rc;
+  GPG_CUDA(cudaSetDevice(device_id));
+  // kernel attributes and occupancy are queried outside the capture
+  if (p->real_size == 4) {
+    BatchLaunchCfg<float> *c;
+    if (int rc = batch_prepare<float>(c)) return rc;
+  } else {
+    BatchLaunchCfg<double> *c;
+    if (int rc = batch_prepare<double>(c)) return rc;
+  }
+  auto *plan = new gpg_batch_plan;
+  plan->device = device_id;
+  auto cleanup = [&](int rc) {
+    gpg_batch_plan_destroy(plan);
+    return rc;
+  };
+  cudaError_t e = cudaMalloc(&plan->d_counter, sizeof(uint32_t));
+  if (e != cudaSuccess) return cleanup(fail(GPG_ERR_OOM, "cudaMalloc counter: %s", cudaGetErrorString(e)));
+  e = cudaStreamCreateWithFlags(&plan->capture, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
+  e = cudaStreamBeginCapture(plan->capture, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e)));
+  int rc = p->real_size == 4 ? solve_batch_typed<float>(*p, ngroup, groups, plan->d_counter, plan->capture)
+                             : solve_batch_typed<double>(*p, ngroup, groups, plan->d_counter, plan->capture);
+  e = cudaStreamEndCapture(plan->capture, &plan->graph);
+  if (rc) return cleanup(rc);
+  if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e)));
+  e = cudaGraphInstantiate(&plan->exec, plan->graph, 0);
+  if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e)));
+  *out = plan;
+  return GPG_OK;
+}
+
+extern "C" int gpg_batch_plan_launch(gpg_batch_plan *plan, void *stream) {
+  if (!plan || !plan->exec) return fail(GPG_ERR_INVALID, "plan is NULL");
+  GPG_CUDA(cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream)));
   return GPG_OK;
 }

@@ -8,7 +8,8 @@
 //        R = phi(z+1)+phi(z-1)+phi(y+1)+phi(y-1)+phi(x+1)+phi(x-1) - 6phi - Const rho
 //        phi += Omega/6 R,   Total += |R|      (Total accumulated in double)
 //      stop after the first sweep whose Total grows once Iter+1 >= Min_Iter
-//      (or, in tolerance mode, once Total <= tol * sum|Const rho|); cap Max_Iter
+//      (or, in tolerance mode, once Total <= tol * sum|Const rho| -- or <= tol
+//      in absolute-tolerance mode); cap Max_Iter
 //   c. copy the GRA_NXT^3 window of the cube to pot_out
 //
 // B200 layout.  A team of 1-4 warps owns a patch.  Lane (y, h) owns the
@@ -131,28 +132,23 @@ __device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2
   for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
 }
 
-// PPC: teams (patches) per CTA.  PHASED: form the M independent updates of a
-// pass phase by phase across heights (more updates in flight, more registers)
-// instead of height by height.  Both orders give identical bits; the
-// autotuner (gpg_set_sor_variant) picks per (precision, ghost size).
-template <typename T, int G, int PPC, bool PHASED>
-__global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
-    sor_kernel(const SolveArgs<T> a) {
+// Solve patch P_ with the team `team` (thread `tid` of TEAM) whose shared
+// memory starts at `tb` (SorSmem::team_bytes).  Used by the per-ghost-size
+// kernel below and by the mixed-size persistent kernel (batch_kernel.cuh),
+// so both produce the same bits for a patch.
+template <typename T, int G, bool PHASED>
+__device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P_, int team, int tid,
+                                                unsigned char *tb) {
   using g = Geo<G>;
   using C = SorCfg<T, G>;
   using S = SorSmem<T, G>;
   constexpr int N = g::N, M = g::M, HALF = g::HALF, TEAM = C::TEAM, NWARP = C::NWARP;
   constexpr int P = C::P, PP = C::PP, R = C::R, CW = C::CW;
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int team = threadIdx.x / TEAM, tid = threadIdx.x - team * TEAM;
+  (void)P;
   const int lane = tid & 31, warp = tid >> 5;
-  unsigned char *tb = smem_raw + team * S::team_bytes;
   T *s_cube = reinterpret_cast<T *>(tb);
   double *s_part = reinterpret_cast<double *>(tb + S::round(S::cube_bytes));
 
-  const int64_t P_ = int64_t(blockIdx.x) * PPC + team;
-  if (P_ >= a.npatch) return;  // whole team leaves together
 
   // ---- interpolate the coarse potential into the cube (reads via L1) -----
   interpolate<T, G, TEAM>(a.pot_in + P_ * g::PN3, tid, a.int_scheme,
@@ -212,6 +208,8 @@ __global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
       for (int w = 1; w < NWARP; ++w) cr_sum += s_part[w];
     }
     tol_abs = a.sor_tol * cr_sum;
+  } else if (a.stop_mode == 2) {
+    tol_abs = a.sor_tol;
   }
   team_sync<TEAM>(team);
 
@@ -279,6 +277,21 @@ __global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
     gravity_patch<T, TEAM>(a.flu + P_ * 5 * 512, tid, a.gra_const, a.p5,
                            [s_cube](int i, int j, int k) { return s_cube[C::addr(i + G, j + G, k + G)]; });
   }
+}
+
+// PPC: teams (patches) per CTA.  PHASED: form the M independent updates of a
+// pass phase by phase across heights (more updates in flight, more registers)
+// instead of height by height.  Both orders give identical bits; the
+// autotuner (gpg_set_sor_variant) picks per (precision, ghost size).
+template <typename T, int G, int PPC, bool PHASED>
+__global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
+    sor_kernel(const SolveArgs<T> a) {
+  constexpr int TEAM = SorCfg<T, G>::TEAM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int team = threadIdx.x / TEAM, tid = threadIdx.x - team * TEAM;
+  const int64_t P_ = int64_t(blockIdx.x) * PPC + team;
+  if (P_ >= a.npatch) return;  // whole team leaves together
+  sor_solve_patch<T, G, PHASED>(a, P_, team, tid, smem_raw + team * SorSmem<T, G>::team_bytes);
 }
 
 }  // namespace gpg

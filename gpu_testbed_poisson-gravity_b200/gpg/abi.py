@@ -15,7 +15,7 @@ GPG_ERR_STATE = 6
 GPG_SOR, GPG_MG = 1, 2
 GPG_INT_CQUAD, GPG_INT_QUAD = 4, 5
 GPG_INIT_INTERP, GPG_INIT_ZERO, GPG_INIT_GUESS = 0, 1, 2
-GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE = 0, 1
+GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE, GPG_STOP_ABS_TOLERANCE = 0, 1, 2
 NULL_INT = 2147483647
 
 
@@ -63,6 +63,23 @@ class GpgParams(C.Structure):
     def dtype(self):
         import numpy as np
         return np.float32 if self.real_size == 4 else np.float64
+
+
+class GpgBatchGroup(C.Structure):
+    """Field-for-field copy of ``struct gpg_batch_group`` in include/gpg.h."""
+
+    _fields_ = [
+        ("ghost", C.c_int32),
+        ("npatch", C.c_int32),
+        ("d_rho", C.c_void_p),
+        ("d_pot_in", C.c_void_p),
+        ("d_pot_out", C.c_void_p),
+        ("d_flu", C.c_void_p),
+        ("d_guess", C.c_void_p),
+        ("d_iters", C.c_void_p),
+        ("d_resid", C.c_void_p),
+        ("sor_omega", C.c_double),
+    ]
 
 
 SOR_OMEGA = {1: 1.49, 2: 1.57, 3: 1.62, 4: 1.65, 5: 1.69}

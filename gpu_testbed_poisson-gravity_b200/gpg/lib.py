@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-from .abi import GPG_OK, GPG_SOR, GpgParams, default_params, patch_sizes  # noqa: F401
+from .abi import GPG_OK, GPG_SOR, GpgBatchGroup, GpgParams, default_params, patch_sizes  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -58,6 +58,14 @@ def library(path: str | None = None):
         "gpg_asyn_poisson_gravity_solver": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, P, C.c_int]),
         "gpg_synchronize": (C.c_int, [vp]),
         "gpg_last_iterations": (C.c_int, [vp, vp, vp, C.c_int]),
+        "gpg_solve_batch_device": (C.c_int, [P, C.c_int, C.POINTER(GpgBatchGroup), vp, vp]),
+        "gpg_batch_plan_create": (C.c_int, [C.POINTER(vp), P, C.c_int, C.POINTER(GpgBatchGroup), C.c_int]),
+        "gpg_batch_plan_launch": (C.c_int, [vp, vp]),
+        "gpg_batch_plan_destroy": (C.c_int, [vp]),
+        "gpg_sor_variant_count": (C.c_int, []),
+        "gpg_sor_variant_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "gpg_set_sor_variant": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+        "gpg_get_sor_variant": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -191,3 +199,58 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---------------------------------------------------------------------------
+# batched mixed-ghost-size SOR
+# ---------------------------------------------------------------------------
+def make_batch_groups(p: GpgParams, groups: list[dict]):
+    """ctypes array of gpg_batch_group from dicts of torch CUDA tensors
+    (keys: ghost, rho, pot_in, pot_out, flu, guess, iters, resid, omega)."""
+    arr = (GpgBatchGroup * max(1, len(groups)))()
+    for i, g in enumerate(groups):
+        a = arr[i]
+        a.ghost = g["ghost"]
+        a.npatch = int(g["rho"].shape[0])
+        for k, f in (("rho", "d_rho"), ("pot_in", "d_pot_in"), ("pot_out", "d_pot_out"), ("flu", "d_flu"),
+                     ("guess", "d_guess"), ("iters", "d_iters"), ("resid", "d_resid")):
+            t = g.get(k)
+            setattr(a, f, None if t is None else _tptr(t).value)
+        a.sor_omega = g.get("omega", 0.0)
+    return arr
+
+
+def solve_batch_device(p: GpgParams, groups: list[dict], counter, stream=None):
+    """One persistent launch over groups of different ghost sizes.  `counter`:
+    a 1-element int32 CUDA tensor used as the work-queue counter."""
+    import torch
+    arr = make_batch_groups(p, groups)
+    s = stream if stream is not None else torch.cuda.current_stream(counter.device)
+    check(library().gpg_solve_batch_device(C.byref(p), len(groups), arr, _tptr(counter),
+                                           C.c_void_p(s.cuda_stream)))
+
+
+class BatchPlan:
+    """The batch captured once into a CUDA graph; launch() replays it."""
+
+    def __init__(self, p: GpgParams, groups: list[dict], device_id: int = 0):
+        self._plan = C.c_void_p()
+        self._keep = groups  # buffers must outlive the graph
+        arr = make_batch_groups(p, groups)
+        check(library().gpg_batch_plan_create(C.byref(self._plan), C.byref(p), len(groups), arr, device_id))
+
+    def launch(self, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        check(library().gpg_batch_plan_launch(self._plan, C.c_void_p(s.cuda_stream)))
+
+    def close(self):
+        if self._plan:
+            check(library().gpg_batch_plan_destroy(self._plan))
+            self._plan = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

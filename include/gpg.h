@@ -55,11 +55,12 @@ enum { GPG_INT_CQUAD = 4, GPG_INT_QUAD = 5 };
  *   GUESS:  interior taken from a caller array [P][RHO_NXT]^3 */
 enum { GPG_INIT_INTERP = 0, GPG_INIT_ZERO = 1, GPG_INIT_GUESS = 2 };
 /* SOR stopping rule.
- *   REFERENCE: stop after the first sweep whose L1 residual grows, once
- *              Iter+1 >= Min_Iter; cap Max_Iter (CPU_PoissonSolver_SOR.cpp:273-283)
- *   TOLERANCE: stop once Iter+1 >= Min_Iter and the sweep's L1 residual
- *              <= sor_tolerance * sum|Poi_Coeff*dh^2*rho|; cap Max_Iter */
-enum { GPG_STOP_REFERENCE = 0, GPG_STOP_TOLERANCE = 1 };
+ *   REFERENCE:     stop after the first sweep whose L1 residual grows, once
+ *                  Iter+1 >= Min_Iter; cap Max_Iter (CPU_PoissonSolver_SOR.cpp:273-283)
+ *   TOLERANCE:     stop once Iter+1 >= Min_Iter and the sweep's L1 residual
+ *                  <= sor_tolerance * sum|Poi_Coeff*dh^2*rho|; cap Max_Iter
+ *   ABS_TOLERANCE: the same with the L1 residual <= sor_tolerance */
+enum { GPG_STOP_REFERENCE = 0, GPG_STOP_TOLERANCE = 1, GPG_STOP_ABS_TOLERANCE = 2 };
 
 /* Runtime form of the reference's compile-time shape (Makefile:13-85) plus the
  * argument list of CUAPI_Asyn_PoissonGravitySolver (Header/Prototype.h:25-34).
@@ -86,7 +87,7 @@ typedef struct gpg_params {
   double poi_coeff;        /* 4*pi*G*a */
   int32_t stop_mode;       /* GPG_STOP_* (SOR only) */
   int32_t reserved0;
-  double sor_tolerance;    /* relative L1 tolerance for GPG_STOP_TOLERANCE */
+  double sor_tolerance;    /* L1 tolerance for GPG_STOP_TOLERANCE (relative) / _ABS_TOLERANCE */
 } gpg_params;
 
 /* Fill `p` with the reference defaults for (real_size, ghost, scheme):
@@ -161,6 +162,43 @@ GPG_API int gpg_synchronize(gpg_context *ctx);
  * copies; valid after gpg_synchronize).  No reference counterpart: the
  * reference only prints them (CPU_PoissonSolver_SOR.cpp:288). */
 GPG_API int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
+
+/* ---------------------------------------------------------------------------
+ * Batched SOR over patches of mixed ghost sizes, one persistent launch.
+ * No single reference counterpart: the reference compiles one ghost size per
+ * build and launches one kernel per stream (CUAPI_Asyn_PoissonGravitySolver.cu:
+ * 206-249).  A group is a set of patches of one ghost size in the reference
+ * layout; `p` supplies everything else (p->ghost is ignored, p->scheme must be
+ * GPG_SOR).  Each patch gives the same bits as gpg_poisson_gravity_device.
+ * ------------------------------------------------------------------------- */
+typedef struct gpg_batch_group {
+  int32_t ghost;        /* POT_GHOST_SIZE of the group, 1..5 */
+  int32_t npatch;
+  const void *d_rho;    /* [npatch][RHO_NXT]^3 */
+  const void *d_pot_in; /* [npatch][POT_NXT]^3 */
+  void *d_pot_out;      /* [npatch][GRA_NXT]^3 */
+  void *d_flu;          /* [npatch][5][8]^3 when p->gra_acc, else may be NULL */
+  const void *d_guess;  /* [npatch][RHO_NXT]^3 when init_mode == GPG_INIT_GUESS */
+  int32_t *d_iters;     /* [npatch] or NULL */
+  double *d_resid;      /* [npatch] or NULL */
+  double sor_omega;     /* omega of the group; <= 0 selects the reference default */
+} gpg_batch_group;
+
+#define GPG_BATCH_MAX_GROUPS 8
+
+/* Stream-ordered.  d_counter: one uint32 of device memory the call resets and
+ * uses as the work-queue counter (calls that overlap need separate counters). */
+GPG_API int gpg_solve_batch_device(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
+                                   uint32_t *d_counter, void *stream);
+
+/* The same batch captured once into a CUDA graph (counter reset + persistent
+ * kernel); gpg_batch_plan_launch replays it on `stream`.  The plan owns its
+ * counter; the group buffers must outlive the plan. */
+typedef struct gpg_batch_plan gpg_batch_plan;
+GPG_API int gpg_batch_plan_create(gpg_batch_plan **plan, const gpg_params *p, int ngroup,
+                                  const gpg_batch_group *groups, int device_id);
+GPG_API int gpg_batch_plan_launch(gpg_batch_plan *plan, void *stream);
+GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
 
 /* ---------------------------------------------------------------------------
  * SOR kernel variants.  No reference counterpart (the reference fixes its

@@ -376,7 +376,7 @@ int FN(oracle_poisson_gravity)(const gpg_params *prm, int npatch, const T *rho_a
                   cube[((size_t)(c + 1) * N + (b + 1)) * N + (a + 1)] =
                      prm->init_mode == GPG_INIT_GUESS
                         ? guess_all[(size_t)P * sr + ((size_t)c * M + b) * M + a] : (T)0.0;
-            double tol_abs = 0.0;
+            double tol_abs = prm->sor_tolerance;  /* GPG_STOP_ABS_TOLERANCE */
             if (prm->stop_mode == GPG_STOP_TOLERANCE) {
                double s = 0.0;
                for (size_t t = 0; t < sr; t++) s += (double)TABS(Const * rho[t]);

@@ -30,9 +30,9 @@ def oracle_lib():
     global _lib
     if _lib is None:
         path = os.path.join(HERE, "liboracle.so")
-        if not os.path.exists(path):
-            from oracle.build import build_oracle  # local build when missing
-            build_oracle()
+        if os.path.exists(os.path.join(HERE, "gpg_oracle.c")):
+            from oracle.build import build_oracle  # rebuilds only when out of date
+            path = build_oracle()
         lib = C.CDLL(path)
         for sfx in ("f32", "f64"):
             f = getattr(lib, f"oracle_poisson_gravity_{sfx}")
