@@ -683,13 +683,14 @@ template <typename T>
 int solve_batch_typed(const gpg_params &p, int ngroup, const gpg_batch_group *groups, uint32_t *counter,
                       cudaStream_t s) {
   gpg::BatchArgs<T> b{};
-  std::vector<int> order(ngroup);
-  std::iota(order.begin(), order.end(), 0);
+  int order[gpg::kBatchMaxGroups];
+  std::iota(order, order + ngroup, 0);
   // largest cubes first: their units are the longest, so they start earliest
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return groups[x].ghost > groups[y].ghost; });
+  std::stable_sort(order, order + ngroup, [&](int x, int y) { return groups[x].ghost > groups[y].ghost; });
   int64_t u = 0;
   int k = 0;
-  for (int idx : order) {
+  for (int n = 0; n < ngroup; ++n) {
+    const int idx = order[n];
     const gpg_batch_group &gr = groups[idx];
     if (gr.npatch == 0) continue;
     gpg_params q = p;
@@ -788,4 +789,62 @@ extern "C" int gpg_batch_plan_launch(gpg_batch_plan *plan, void *stream) {
   if (!plan || !plan->exec) return fail(GPG_ERR_INVALID, "plan is NULL");
   GPG_CUDA(cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream)));
   return GPG_OK;
+}
+
+// ===========================================================================
+// batched SOR without any allocation by the library or the caller
+// ===========================================================================
+// For callers that may not allocate device memory when they solve: codes that
+// hand all device memory to their own pool up front, solves issued while
+// another runtime holds the allocator, or a fixed memory budget that must not
+// move between steps.  The batch kernel's only scratch, its work-queue
+// counter, lives here in a static device array instead of a caller buffer.
+// Every GPU that loads libgpg holds this array until the process exits; all
+// calls on one device share it.
+namespace {
+
+static __device__ __align__(256) unsigned int g_noalloc_queue[GPG_BATCH_NOALLOC_SCRATCH_WORDS];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned int *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_queue on the current device.  In host code the
+// array's name only stands in for the symbol, so the address is looked up
+// once per device (with that device current) and cached.
+int noalloc_scratch(unsigned int **out) {
+  int dev = 0;
+  GPG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(GPG_ERR_UNSUPPORTED, "device %d: at most %d devices supported", dev, kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_queue);
+    if (e != cudaSuccess || ptr == nullptr)
+      return fail(GPG_ERR_CUDA, "cudaGetSymbolAddress(work-queue scratch): %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<unsigned int *>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return GPG_OK;
+}
+
+}  // namespace
+
+extern "C" int gpg_solve_batch_device_noalloc(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
+                                              void *stream) {
+  if (int rc = validate_batch(p, ngroup, groups)) return rc;
+  int64_t total = 0;
+  for (int i = 0; i < ngroup; ++i) total += groups[i].npatch;
+  if (total > GPG_BATCH_NOALLOC_MAX_PATCHES)
+    return fail(GPG_ERR_INVALID,
+                "batch of %lld patches exceeds the %lld that one call without allocation may queue "
+                "(its work-queue counter is a single 32-bit word)",
+                (long long)total, (long long)GPG_BATCH_NOALLOC_MAX_PATCHES);
+  unsigned int *counter = nullptr;
+  if (int rc = noalloc_scratch(&counter)) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the counter is reset to zero on `stream` before the kernel reads it
+  return p->real_size == 4 ? solve_batch_typed<float>(*p, ngroup, groups, counter, s)
+                           : solve_batch_typed<double>(*p, ngroup, groups, counter, s);
 }

@@ -191,6 +191,28 @@ typedef struct gpg_batch_group {
 GPG_API int gpg_solve_batch_device(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
                                    uint32_t *d_counter, void *stream);
 
+/* Allocation-free variant of gpg_solve_batch_device.  No counterpart in the
+ * reference.  Some callers cannot allocate device memory at the point where
+ * they solve -- a code that gives all device memory to its own pool at start-
+ * up, one whose allocator belongs to another runtime, or one that must keep a
+ * fixed memory footprint between time steps -- so this entry point needs no
+ * buffer beyond the caller's inputs and outputs and calls no cudaMalloc or
+ * cudaFree: the work-queue counter lives in a static device array inside
+ * libgpg (GPG_BATCH_NOALLOC_SCRATCH_WORDS words, 256-byte aligned, held on
+ * every GPU that loads the library until the process exits).
+ *  - The first call on a device looks up that array's device address
+ *    (cudaGetSymbolAddress) and caches it; make that first call before any
+ *    stream capture on the device.
+ *  - The counter is reset on `stream` at the start of every call, but all
+ *    calls on a device share it: calls whose work overlaps on the GPU (other
+ *    streams, other host threads) race and must be serialised by the caller.
+ *  - At most GPG_BATCH_NOALLOC_MAX_PATCHES patches per call; larger batches
+ *    are rejected with GPG_ERR_INVALID. */
+#define GPG_BATCH_NOALLOC_SCRATCH_WORDS 1
+#define GPG_BATCH_NOALLOC_MAX_PATCHES (1LL << 30)
+GPG_API int gpg_solve_batch_device_noalloc(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
+                                           void *stream);
+
 /* The same batch captured once into a CUDA graph (counter reset + persistent
  * kernel); gpg_batch_plan_launch replays it on `stream`.  The plan owns its
  * counter; the group buffers must outlive the plan. */
