@@ -165,6 +165,115 @@ def _run_cpu(kind, p, d, n, nthreads):
 
 
 # ---------------------------------------------------------------------------
+# other BASELINE configurations, measured beside the headline (not the bench value)
+# ---------------------------------------------------------------------------
+def _event_ms(torch, fn, reps=5, warm=3):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def extra_configs(torch, dev, cpu: bool):
+    """MG + 5-point gravity (16384 patches, ghost 3, FP32); the mixed batch
+    (65536 patches, ghost 1-5 in 30/30/20/10/10 %, rho0 log-uniform over 4
+    decades, zero start, absolute L1 tolerance, one persistent launch replayed
+    from a CUDA graph); plain SOR from zero start to a fixed relative
+    tolerance (the plain-SOR arm of the metric)."""
+    from gpg.abi import GPG_INIT_ZERO, GPG_MG, GPG_STOP_ABS_TOLERANCE, GPG_STOP_TOLERANCE
+    from gpg.inputs import log_uniform, mixed_ghost_assignment
+    from gpg.lib import BatchPlan, solve_device
+    out = {}
+    # --- MG + P5 gravity -----------------------------------------------------
+    n = 16384
+    d = make_patches(n, 3, seed=21, gra_ghost=2, dtype=np.float32)
+    p = default_params(4, 3, 2, gra_ghost=2, p5_gradient=1)
+    t = {k: torch.from_numpy(v).to(dev) for k, v in d.items() if k != "geometry"}
+    pot = torch.empty((n, 12, 12, 12), device=dev)
+    it = torch.empty(n, dtype=torch.int32, device=dev)
+    rs = torch.empty(n, dtype=torch.float64, device=dev)
+    flu = t["flu"].clone()
+    ms = _event_ms(torch, lambda: solve_device(p, t["rho"], t["pot_in"], pot_out=pot, flu=flu, iters=it, resid=rs))
+    rec = {"workload": "MG V-cycle, ghost 3, FP32 (FP64 error norm), 5-point gravity, 16384 patches",
+           "patches_per_s": n / ms * 1e3, "ms": ms, "cycles_mean": float(it.float().mean())}
+    if cpu:
+        from oracle.oracle import ref_available, run_reference
+        if ref_available("mg", 3, 2, "f32"):
+            m = 2048
+            t0 = time.perf_counter()
+            run_reference(p, np.ascontiguousarray(d["rho"][:m]), d["pot_in"][:m].copy(), flu=d["flu"][:m].copy())
+            rec["cpu_reference_patches_per_s"] = m / (time.perf_counter() - t0)
+    out["mg_gravity_g3_f32_16384"] = rec
+    # --- mixed batch ---------------------------------------------------------
+    N = 65536
+    gh = mixed_ghost_assignment(N, 7)
+    rho0 = log_uniform(N, 8)
+    groups, crsum = [], 0.0
+    for g in range(1, 6):
+        idx = np.flatnonzero(gh == g)
+        dd = make_patches(len(idx), g, seed=100 + g, rho0=rho0[idx], dtype=np.float32, fluid=False)
+        cr = np.abs(dd["rho"].astype(np.float64)).reshape(len(idx), -1).sum(1).max() * 4 * np.pi * 1e-5
+        crsum = max(crsum, cr)
+        m = len(idx)
+        groups.append({"ghost": g, "rho": torch.from_numpy(dd["rho"]).to(dev),
+                       "pot_in": torch.from_numpy(dd["pot_in"]).to(dev),
+                       "pot_out": torch.empty((m, 10, 10, 10), device=dev),
+                       "iters": torch.empty(m, dtype=torch.int32, device=dev),
+                       "resid": torch.empty(m, dtype=torch.float64, device=dev)})
+    # absolute tolerance: 3 % of the largest patch's L1 source norm, just above the
+    # FP32 round-off floor of the densest patches (0.6-1.8 % of that norm)
+    tol = 0.03 * crsum
+    pb = default_params(4, 1, GPG_SOR, init_mode=GPG_INIT_ZERO, stop_mode=GPG_STOP_ABS_TOLERANCE,
+                        sor_tolerance=tol, sor_min_iter=1, sor_max_iter=200, gra_acc=0)
+    plan = BatchPlan(pb, groups, dev.index, mode=0)
+    ms = _event_ms(torch, lambda: plan.launch())
+    its = np.concatenate([g["iters"].cpu().numpy() for g in groups])
+    plan.close()
+    plan = BatchPlan(pb, groups, dev.index, mode=1)
+    ms_conc = _event_ms(torch, lambda: plan.launch())
+
+    def separate():
+        for g in groups:
+            q = pb.copy(ghost=g["ghost"], sor_omega={1: 1.49, 2: 1.57, 3: 1.62, 4: 1.65, 5: 1.69}[g["ghost"]])
+            solve_device(q, g["rho"], g["pot_in"], pot_out=g["pot_out"], iters=g["iters"], resid=g["resid"])
+    ms_sep = _event_ms(torch, separate)
+    plan.close()
+    out["batch_mixed_65536_f32"] = {
+        "workload": "65536 patches, ghost 1-5 (30/30/20/10/10 %), rho0 log-uniform 1..1e4, zero start, "
+                    f"L1 residual <= {tol:.4g} (3 % of the largest source norm), one CUDA-graph launch (faster of "
+                    "the persistent work-queue kernel and the concurrent per-ghost-size kernels)",
+        "patches_per_s": N / min(ms, ms_conc) * 1e3, "ms_graph_persistent_work_queue": ms,
+        "ms_graph_concurrent_per_ghost_kernels": ms_conc, "ms_one_launch_per_ghost_size": ms_sep,
+        "iters_min": int(its.min()), "iters_p50": float(np.median(its)), "iters_max": int(its.max()),
+        "frac_max_iter": float((its >= 200).mean())}
+    # --- plain SOR, zero start, fixed relative tolerance ---------------------
+    tot_ms, tot_n = 0.0, 0
+    per = {}
+    for rs_, tolr in ((4, 0.02), (8, 5e-11)):
+        for g in GHOSTS:
+            dd = make_patches(NPATCH, g, seed=1000 + g, dtype=np.float32 if rs_ == 4 else np.float64, fluid=False)
+            pp = default_params(rs_, g, GPG_SOR, init_mode=GPG_INIT_ZERO, stop_mode=GPG_STOP_TOLERANCE,
+                                sor_tolerance=tolr, sor_min_iter=1, sor_max_iter=300, gra_acc=0)
+            tt = {k: torch.from_numpy(v).to(dev) for k, v in dd.items() if k != "geometry"}
+            po = torch.empty((NPATCH, 10, 10, 10), device=dev, dtype=torch.float32 if rs_ == 4 else torch.float64)
+            ms = _event_ms(torch, lambda: solve_device(pp, tt["rho"], tt["pot_in"], pot_out=po, iters=it[:NPATCH],
+                                                       resid=rs[:NPATCH]))
+            per[f"f{8 * rs_}_g{g}"] = {"ms": ms, "iters_mean": float(it[:NPATCH].float().mean())}
+            tot_ms += ms
+            tot_n += NPATCH
+    out["plain_sor_zero_start_rel_tol"] = {
+        "workload": "ghost 2-5 x 4096 patches x FP32/FP64, zero interior start, stop at L1 residual <= "
+                    "0.02 (FP32) / 5e-11 (FP64) x L1 source norm", "patches_per_s": tot_n / tot_ms * 1e3,
+        "per_batch": per}
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +282,7 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other BASELINE configurations")
     ap.add_argument("--only", default=None,
                     help="comma list of batches to run (e.g. f64_g5); profiling cases, not a bench line")
     a = ap.parse_args(argv)
@@ -296,9 +406,17 @@ def main(argv=None) -> int:
             e2e_s = float(t.item())
         h2d = step_inputs
         d2h = sum(NPATCH * (patch_sizes(p)["pot_out"] * p.real_size + 4 + 8) for p, _ in batches)
+        # host link: pinned -> device copy bandwidth, the bound of this leg
+        hb = torch.empty(256 * 2 ** 20, dtype=torch.uint8).pin_memory()
+        db = torch.empty_like(hb, device=dev)
+        link_ms = _event_ms(torch, lambda: db.copy_(hb, non_blocking=True), reps=5, warm=2)
+        link_gbs = hb.numel() / (link_ms / 1e3) / 1e9
+        del hb, db
         e2e = {"value": world * patches_step * a.steps / e2e_s, "unit": "patches/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "timing": "host clock around full device sync"}
+               "timing": "host clock around full device sync",
+               "h2d_link_gbs": link_gbs,
+               "h2d_bound_patches_per_s": world * patches_step / (h2d / (link_gbs * 1e9))}
         for c in ctxs:
             c.close()
 
@@ -347,6 +465,8 @@ def main(argv=None) -> int:
     if rank == 0 and not a.no_cpu_baseline and world == 1:
         v, cores, kind, sample = reference_cpu(batches, budget_s=20.0)
         line["cpu_baseline"] = {"value": v, "unit": "patches/s", "cores": cores, "kind": kind, "sample": sample}
+    if rank == 0 and not a.no_extra and not a.only and world == 1:
+        line["extra"] = extra_configs(torch, dev, cpu=not a.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

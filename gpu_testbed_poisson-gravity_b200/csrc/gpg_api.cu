@@ -115,12 +115,18 @@ void load_tune_file() {
 }
 
 template <typename T, int G, int PPC, bool PHASED>
+AttrOnce &sor_attr() {
+  static AttrOnce attr;
+  return attr;
+}
+
+template <typename T, int G, int PPC, bool PHASED>
 int launch_sor_v(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   using S = gpg::SorSmem<T, G>;
   const size_t smem = PPC * S::team_bytes;
   if (smem > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %zu bytes of shared memory", smem);
   auto fn = gpg::sor_kernel<T, G, PPC, PHASED>;
-  static AttrOnce attr;
+  AttrOnce &attr = sor_attr<T, G, PPC, PHASED>();
   if (int rc = ensure_smem(fn, smem, attr)) return rc;
   if (PPC * gpg::SorCfg<T, G>::TEAM > attr.max_threads)
     return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %d threads per CTA (registers allow %d)",
@@ -129,6 +135,15 @@ int launch_sor_v(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   fn<<<(unsigned)grid, PPC * gpg::SorCfg<T, G>::TEAM, smem, s>>>(a);
   GPG_CUDA(cudaGetLastError());
   return GPG_OK;
+}
+
+// Kernel attributes of the SOR variant a (precision, ghost) solve will launch,
+// set without launching (stream capture must not see first-use set-up).
+template <typename T, int G, int PPC, bool PHASED>
+int prepare_sor_v() {
+  auto fn = gpg::sor_kernel<T, G, PPC, PHASED>;
+  static AttrOnce &attr = sor_attr<T, G, PPC, PHASED>();
+  return ensure_smem(fn, PPC * gpg::SorSmem<T, G>::team_bytes, attr);
 }
 
 template <typename T, int G>
@@ -142,6 +157,36 @@ int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
     case 4: return launch_sor_v<T, G, 4, false>(a, s);
     default: return launch_sor_v<T, G, 4, true>(a, s);
   }
+}
+
+template <typename T, int G>
+int prepare_sor() {
+  std::call_once(g_tune_once, load_tune_file);
+  switch (g_sor_variant[sizeof(T) == 8][G]) {
+    case 0: return prepare_sor_v<T, G, 1, false>();
+    case 1: return prepare_sor_v<T, G, 1, true>();
+    case 2: return prepare_sor_v<T, G, 2, false>();
+    case 3: return prepare_sor_v<T, G, 2, true>();
+    case 4: return prepare_sor_v<T, G, 4, false>();
+    default: return prepare_sor_v<T, G, 4, true>();
+  }
+}
+
+template <typename T>
+int prepare_sor_typed(int ghost) {
+  switch (ghost) {
+    case 1: return prepare_sor<T, 1>();
+    case 2: return prepare_sor<T, 2>();
+    case 3: return prepare_sor<T, 3>();
+    case 4: return prepare_sor<T, 4>();
+    default: return prepare_sor<T, 5>();
+  }
+}
+
+// Attributes of the SOR kernel a solve with `q` launches (stream capture must
+// not be the first use of a kernel).
+int prepare_solve_kernels(const gpg_params &q) {
+  return q.real_size == 4 ? prepare_sor_typed<float>(q.ghost) : prepare_sor_typed<double>(q.ghost);
 }
 
 template <typename T, int G>
@@ -733,9 +778,34 @@ struct gpg_batch_plan {
   int device = 0;
   uint32_t *d_counter = nullptr;
   cudaStream_t capture = nullptr;
+  cudaStream_t branch[GPG_BATCH_MAX_GROUPS] = {};
+  cudaEvent_t fork = nullptr, join[GPG_BATCH_MAX_GROUPS] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
+
+namespace {
+// Per-ghost-size kernels of a batch as parallel branches of the capture:
+// fork from `main`, one branch stream per group, join back.
+int capture_concurrent(gpg_batch_plan *plan, const gpg_params *p, int ngroup, const gpg_batch_group *groups) {
+  GPG_CUDA(cudaEventRecord(plan->fork, plan->capture));
+  for (int i = 0; i < ngroup; ++i) {
+    const gpg_batch_group &g = groups[i];
+    GPG_CUDA(cudaStreamWaitEvent(plan->branch[i], plan->fork, 0));
+    if (g.npatch > 0) {
+      gpg_params q = *p;
+      q.ghost = g.ghost;
+      q.sor_omega = g.sor_omega > 0 ? g.sor_omega : kDefaultOmega[g.ghost - 1];
+      if (int rc = gpg_poisson_gravity_device(&q, g.npatch, g.d_rho, g.d_pot_in, g.d_pot_out, g.d_flu, g.d_guess,
+                                              g.d_iters, g.d_resid, plan->branch[i]))
+        return rc;
+    }
+    GPG_CUDA(cudaEventRecord(plan->join[i], plan->branch[i]));
+    GPG_CUDA(cudaStreamWaitEvent(plan->capture, plan->join[i], 0));
+  }
+  return GPG_OK;
+}
+}  // namespace
 
 extern "C" int gpg_batch_plan_destroy(gpg_batch_plan *plan) {
   if (!plan) return GPG_OK;
@@ -743,17 +813,35 @@ extern "C" int gpg_batch_plan_destroy(gpg_batch_plan *plan) {
   if (plan->exec) cudaGraphExecDestroy(plan->exec);
   if (plan->graph) cudaGraphDestroy(plan->graph);
   if (plan->capture) cudaStreamDestroy(plan->capture);
+  for (int i = 0; i < GPG_BATCH_MAX_GROUPS; ++i) {
+    if (plan->branch[i]) cudaStreamDestroy(plan->branch[i]);
+    if (plan->join[i]) cudaEventDestroy(plan->join[i]);
+  }
+  if (plan->fork) cudaEventDestroy(plan->fork);
   if (plan->d_counter) cudaFree(plan->d_counter);
   delete plan;
   return GPG_OK;
 }
 
 extern "C" int gpg_batch_plan_create(gpg_batch_plan **out, const gpg_params *p, int ngroup,
-                                     const gpg_batch_group *groups, int device_id) {
+                                     const gpg_batch_group *groups, int device_id, int mode) {
   if (!out) return fail(GPG_ERR_INVALID, "plan is NULL");
   *out = nullptr;
+  if (mode != GPG_PLAN_PERSISTENT && mode != GPG_PLAN_CONCURRENT) return fail(GPG_ERR_INVALID, "mode %d", mode);
   if (int rc = validate_batch(p, ngroup, groups)) return rc;
   GPG_CUDA(cudaSetDevice(device_id));
+  if (mode == GPG_PLAN_CONCURRENT) {
+    // every kernel the branches launch gets its attributes outside the capture
+    for (int i = 0; i < ngroup; ++i) {
+      if (groups[i].npatch == 0) continue;
+      gpg_params q = *p;
+      q.ghost = groups[i].ghost;
+      if (int rc = gpg_poisson_gravity_device(&q, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                              nullptr, nullptr))
+        return rc;  // npatch 0: validates only
+      if (int rc = prepare_solve_kernels(q)) return rc;
+    }
+  }
   // kernel attributes and occupancy are queried outside the capture
   if (p->real_size == 4) {
     BatchLaunchCfg<float> *c;
@@ -772,10 +860,22 @@ extern "C" int gpg_batch_plan_create(gpg_batch_plan **out, const gpg_params *p, 
   if (e != cudaSuccess) return cleanup(fail(GPG_ERR_OOM, "cudaMalloc counter: %s", cudaGetErrorString(e)));
   e = cudaStreamCreateWithFlags(&plan->capture, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
+  if (mode == GPG_PLAN_CONCURRENT) {
+    e = cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming);
+    for (int i = 0; e == cudaSuccess && i < ngroup; ++i) {
+      e = cudaStreamCreateWithFlags(&plan->branch[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&plan->join[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "plan streams: %s", cudaGetErrorString(e)));
+  }
   e = cudaStreamBeginCapture(plan->capture, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e)));
-  int rc = p->real_size == 4 ? solve_batch_typed<float>(*p, ngroup, groups, plan->d_counter, plan->capture)
-                             : solve_batch_typed<double>(*p, ngroup, groups, plan->d_counter, plan->capture);
+  int rc;
+  if (mode == GPG_PLAN_CONCURRENT)
+    rc = capture_concurrent(plan, p, ngroup, groups);
+  else
+    rc = p->real_size == 4 ? solve_batch_typed<float>(*p, ngroup, groups, plan->d_counter, plan->capture)
+                           : solve_batch_typed<double>(*p, ngroup, groups, plan->d_counter, plan->capture);
   e = cudaStreamEndCapture(plan->capture, &plan->graph);
   if (rc) return cleanup(rc);
   if (e != cudaSuccess) return cleanup(fail(GPG_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e)));

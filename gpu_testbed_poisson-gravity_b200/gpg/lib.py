@@ -59,7 +59,8 @@ def library(path: str | None = None):
         "gpg_synchronize": (C.c_int, [vp]),
         "gpg_last_iterations": (C.c_int, [vp, vp, vp, C.c_int]),
         "gpg_solve_batch_device": (C.c_int, [P, C.c_int, C.POINTER(GpgBatchGroup), vp, vp]),
-        "gpg_batch_plan_create": (C.c_int, [C.POINTER(vp), P, C.c_int, C.POINTER(GpgBatchGroup), C.c_int]),
+        "gpg_batch_plan_create": (C.c_int, [C.POINTER(vp), P, C.c_int, C.POINTER(GpgBatchGroup), C.c_int,
+                                            C.c_int]),
         "gpg_batch_plan_launch": (C.c_int, [vp, vp]),
         "gpg_batch_plan_destroy": (C.c_int, [vp]),
         "gpg_sor_variant_count": (C.c_int, []),
@@ -230,14 +231,20 @@ def solve_batch_device(p: GpgParams, groups: list[dict], counter, stream=None):
                                            C.c_void_p(s.cuda_stream)))
 
 
-class BatchPlan:
-    """The batch captured once into a CUDA graph; launch() replays it."""
+PLAN_PERSISTENT, PLAN_CONCURRENT = 0, 1
 
-    def __init__(self, p: GpgParams, groups: list[dict], device_id: int = 0):
+
+class BatchPlan:
+    """The batch captured once into a CUDA graph; launch() replays it.
+    mode PLAN_PERSISTENT: the work-queue kernel; PLAN_CONCURRENT: the
+    per-ghost-size kernels as parallel graph branches."""
+
+    def __init__(self, p: GpgParams, groups: list[dict], device_id: int = 0, mode: int = PLAN_PERSISTENT):
         self._plan = C.c_void_p()
         self._keep = groups  # buffers must outlive the graph
         arr = make_batch_groups(p, groups)
-        check(library().gpg_batch_plan_create(C.byref(self._plan), C.byref(p), len(groups), arr, device_id))
+        check(library().gpg_batch_plan_create(C.byref(self._plan), C.byref(p), len(groups), arr, device_id,
+                                              mode))
 
     def launch(self, stream=None):
         import torch

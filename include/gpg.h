@@ -213,12 +213,16 @@ GPG_API int gpg_solve_batch_device(const gpg_params *p, int ngroup, const gpg_ba
 GPG_API int gpg_solve_batch_device_noalloc(const gpg_params *p, int ngroup, const gpg_batch_group *groups,
                                            void *stream);
 
-/* The same batch captured once into a CUDA graph (counter reset + persistent
- * kernel); gpg_batch_plan_launch replays it on `stream`.  The plan owns its
+/* The same batch captured once into a CUDA graph; gpg_batch_plan_launch
+ * replays it on `stream`.  mode GPG_PLAN_PERSISTENT: counter reset + the
+ * persistent work-queue kernel.  mode GPG_PLAN_CONCURRENT: one per-ghost-size
+ * kernel per group as parallel branches of the graph, so the hardware block
+ * scheduler interleaves their CTAs (same bits either way).  The plan owns its
  * counter; the group buffers must outlive the plan. */
+enum { GPG_PLAN_PERSISTENT = 0, GPG_PLAN_CONCURRENT = 1 };
 typedef struct gpg_batch_plan gpg_batch_plan;
 GPG_API int gpg_batch_plan_create(gpg_batch_plan **plan, const gpg_params *p, int ngroup,
-                                  const gpg_batch_group *groups, int device_id);
+                                  const gpg_batch_group *groups, int device_id, int mode);
 GPG_API int gpg_batch_plan_launch(gpg_batch_plan *plan, void *stream);
 GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
 

@@ -83,21 +83,28 @@ def test_batch_matches_oracle(torch):
         assert np.array_equal(g["pot_out"].cpu().numpy()[same], op[same])
 
 
-def test_batch_plan_graph_replay(torch):
-    from gpg.lib import BatchPlan
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_plan_graph_replay(torch, mode):
+    from gpg.lib import BatchPlan, solve_batch_device
     dev = torch.device("cuda:0")
     p = default_params(4, 1, GPG_SOR, gra_acc=0)
     groups, _ = build_groups(torch, 4, 150, seed=5, gra_acc=False, dev=dev)
-    plan = BatchPlan(p, groups)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    solve_batch_device(p, groups, counter)
+    torch.cuda.synchronize()
+    want = [g["pot_out"].clone() for g in groups]
+    plan = BatchPlan(p, groups, mode=mode)
+    for g in groups:
+        g["pot_out"].zero_()
     plan.launch()
     torch.cuda.synchronize()
-    first = [g["pot_out"].clone() for g in groups]
+    assert all(torch.equal(a, g["pot_out"]) for a, g in zip(want, groups))
     for g in groups:
         g["pot_out"].zero_()
     plan.launch()
     plan.launch()
     torch.cuda.synchronize()
-    assert all(torch.equal(a, g["pot_out"]) for a, g in zip(first, groups))
+    assert all(torch.equal(a, g["pot_out"]) for a, g in zip(want, groups))
     plan.close()
 
 
