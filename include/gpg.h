@@ -239,6 +239,36 @@ GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased)
 GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
 GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
 
+/* ---------------------------------------------------------------------------
+ * Learned initial guess for ghost-size-1 SOR (GPG_INIT_GUESS).  No reference
+ * counterpart.  A 4-layer 3^3 convolution network (8 -> 32 -> 32 -> 32 -> 16
+ * channels, ReLU; BF16 weights and activations, FP32 accumulation on the
+ * tcgen05 tensor cores) maps a patch's density and interpolated boundary shell
+ * to its 8^3 interior potential.  Inputs are FP32 ghost-1 arrays: rho
+ * [P][8]^3 and pot_in [P][8]^3; `cnst` is Poi_Coeff*dh^2.  Parameters are one
+ * FP32 vector: per layer W[27][cin][cout] then b[cout] (cin 8 for layer 1 of
+ * which 3 used, cout 16 for layer 4 of which 1 used).
+ * ------------------------------------------------------------------------- */
+typedef struct gpg_net gpg_net;
+GPG_API int gpg_net_create(gpg_net **net, int max_batch, uint64_t seed, int device_id);
+GPG_API int gpg_net_destroy(gpg_net *net);
+GPG_API int gpg_net_param_count(int64_t *count);
+GPG_API int gpg_net_get_params(gpg_net *net, float *host_params);
+GPG_API int gpg_net_set_params(gpg_net *net, const float *host_params);
+/* interior guess [P][8]^3 for GPG_INIT_GUESS (stream-ordered) */
+GPG_API int gpg_net_predict(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in, float *d_guess,
+                            double cnst, void *stream);
+/* loss = mean (net / s - target / s)^2 over interior cells and its gradient
+ * wrt every parameter (d_grad, same layout as the parameters; may be NULL) */
+GPG_API int gpg_net_gradients(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in,
+                              const float *d_target, double cnst, float *d_grad, float *d_loss, void *stream);
+/* gradients + one Adam step (beta 0.9 / 0.999, eps 1e-8) */
+GPG_API int gpg_net_train_step(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in,
+                               const float *d_target, double cnst, float lr, float *d_loss, void *stream);
+/* GPG_ERR_CUDA when a tensor-core wait timed out in an earlier call */
+GPG_API int gpg_net_check(gpg_net *net);
+GPG_API const char *gpg_net_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

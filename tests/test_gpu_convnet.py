@@ -1,0 +1,102 @@
+"""Learned initial guess: tensor-core network vs its FP64 oracle (needs a B200).
+
+The oracle (oracle/convnet_oracle.py) rounds to bfloat16 where the kernels
+store bfloat16; what remains are FP32-vs-FP64 accumulation differences, so the
+checks are relative L2 errors (tolerances stated per test)."""
+import numpy as np
+import pytest
+
+from gpg.inputs import make_patches
+
+pytestmark = pytest.mark.gpu
+CNST = np.float32(4 * np.pi * 1e-5)  # Poi_Coeff * dh^2 in float
+
+
+@pytest.fixture(scope="module")
+def torch():
+    t = pytest.importorskip("torch")
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+def _data(n, seed):
+    d = make_patches(n, 1, seed=seed, fluid=False)
+    rng = np.random.default_rng(seed)
+    target = (d["pot_in"][:, :, :, :].mean() * (1 + 0.1 * rng.standard_normal((n, 8, 8, 8)))).astype(np.float32)
+    return d["rho"], d["pot_in"], target
+
+
+def _oracle_inputs(rho, pot_in):
+    from oracle.oracle import interp_cube
+    from oracle.convnet_oracle import make_input
+    cubes = np.stack([interp_cube(p, 1, 4) for p in pot_in])
+    return make_input(rho, cubes, CNST)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
+
+
+def test_forward_matches_oracle(torch):
+    from gpg.net import Net, split_params
+    from oracle.convnet_oracle import forward
+    rho, pin, _ = _data(3, 11)
+    net = Net(max_batch=4, seed=3)
+    ws, bs = split_params(net.params().astype(np.float64))
+    guess = torch.empty((3, 8, 8, 8), device="cuda")
+    net.predict(torch.from_numpy(rho).cuda(), torch.from_numpy(pin).cuda(), guess, float(CNST))
+    torch.cuda.synchronize()
+    net.check()
+    x0, s = _oracle_inputs(rho, pin)
+    _, y4 = forward(x0, ws, bs)
+    want = y4[:, 1:-1, 1:-1, 1:-1, 0] * s[:, None, None, None]
+    assert rel(guess.cpu().numpy(), want) < 1e-2
+    net.close()
+
+
+def test_gradients_match_oracle(torch):
+    from gpg.net import Net, split_params
+    from oracle.convnet_oracle import loss_and_grads
+    rho, pin, tgt = _data(2, 21)
+    net = Net(max_batch=2, seed=5)
+    p = net.params()
+    ws, bs = split_params(p.astype(np.float64))
+    grad = torch.empty(net.nparams, device="cuda")
+    loss = torch.empty(1, device="cuda")
+    net.gradients(torch.from_numpy(rho).cuda(), torch.from_numpy(pin).cuda(), torch.from_numpy(tgt).cuda(),
+                  float(CNST), grad=grad, loss=loss)
+    torch.cuda.synchronize()
+    net.check()
+    x0, s = _oracle_inputs(rho, pin)
+    ol, odw, odb = loss_and_grads(x0, ws, bs, tgt, s)
+    assert abs(loss.item() - ol) <= 1e-3 * abs(ol)
+    gws, gbs = split_params(grad.cpu().numpy().astype(np.float64))
+    for l in range(4):
+        assert rel(gws[l], odw[l]) < 2e-2, (l, rel(gws[l], odw[l]))
+        assert rel(gbs[l], odb[l]) < 2e-2, (l, rel(gbs[l], odb[l]))
+    net.close()
+
+
+def test_training_reduces_loss(torch):
+    from gpg.net import Net
+    d = make_patches(64, 1, seed=31, fluid=False)
+    from gpg.abi import GPG_INIT_ZERO, GPG_SOR, GPG_STOP_TOLERANCE, default_params
+    from gpg.lib import solve_device
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    p = default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=GPG_INIT_ZERO,
+                       stop_mode=GPG_STOP_TOLERANCE, sor_tolerance=0.02, sor_min_iter=1, sor_max_iter=200)
+    pot, _, _, _ = solve_device(p, rho, pin)          # GRA window = the 8^3 interior
+    target = pot.contiguous()
+    net = Net(max_batch=64, seed=7)
+    loss = torch.empty(1, device="cuda")
+    first = None
+    for it in range(60):
+        net.train_step(rho, pin, target, float(CNST), 1e-3, loss=loss)
+        if first is None:
+            torch.cuda.synchronize()
+            first = loss.item()
+    torch.cuda.synchronize()
+    net.check()
+    assert loss.item() < 0.5 * first
+    net.close()
