@@ -19,6 +19,7 @@
 #include "../../include/gpg.h"
 #include "common.cuh"
 #include "convnet_kernels.cuh"
+#include "convnet_infer.cuh"
 #include "interp.cuh"
 
 using gpg::net::ConvArgs;
@@ -562,6 +563,34 @@ extern "C" int gpg_net_check(gpg_net *n) {
 
 extern "C" int gpg_net_predict(gpg_net *n, int npatch, const float *d_rho, const float *d_pot_in, float *d_guess,
                                double cnst, void *stream) {
+  if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
+  if (npatch < 0) return nfail(GPG_ERR_INVALID, "npatch %d", npatch);
+  if (npatch && (!d_rho || !d_pot_in || !d_guess)) return nfail(GPG_ERR_INVALID, "NULL array");
+  if (!npatch) return GPG_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  static std::once_flag once;
+  static cudaError_t err = cudaSuccess;
+  using gpg::net::InferSmem;
+  if (int rc = set_attr_once(gpg::net::net_infer_kernel, InferSmem::bytes, once, err)) return rc;
+  gpg::net::InferArgs a{};
+  a.rho = d_rho;
+  a.pot_in = d_pot_in;
+  a.guess = d_guess;
+  for (int l = 0; l < kLayers; ++l) {
+    a.w[l] = n->wf[l];
+    a.bias[l] = n->params + param_offset_b(l);
+  }
+  a.cnst = float(cnst);
+  a.npatch = npatch;
+  a.err = n->err;
+  const int grid = std::min(npatch, sm_count());  // persistent: one CTA per SM (shared memory bound)
+  gpg::net::net_infer_kernel<<<grid, gpg::net::kInferThreads, InferSmem::bytes, s>>>(a);
+  NET_CUDA(cudaGetLastError());
+  return GPG_OK;
+}
+
+extern "C" int gpg_net_predict_layers(gpg_net *n, int npatch, const float *d_rho, const float *d_pot_in,
+                                      float *d_guess, double cnst, void *stream) {
   if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
   if (npatch < 0) return nfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch && (!d_rho || !d_pot_in || !d_guess)) return nfail(GPG_ERR_INVALID, "NULL array");

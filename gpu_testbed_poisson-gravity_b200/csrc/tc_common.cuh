@@ -100,10 +100,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity`; returns false (and sets *err) on timeout.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for phase `parity`: gives up after about one second (or 2^26
+// polls); returns false (and sets *err) on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
-  for (uint32_t i = 0; i < (1u << 24); ++i)
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1; i < (1u << 26); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255u) == 0u && globaltimer_ns() - t0 > 1000000000ull) break;
+  }
   if (err) atomicExch(err, 1);
   return false;
 }

@@ -21,6 +21,7 @@ def _net_lib():
             "gpg_net_get_params": (C.c_int, [vp, vp]),
             "gpg_net_set_params": (C.c_int, [vp, vp]),
             "gpg_net_predict": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp]),
+            "gpg_net_predict_layers": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp]),
             "gpg_net_gradients": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp]),
             "gpg_net_train_step": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, C.c_float, vp, vp]),
             "gpg_net_check": (C.c_int, [vp]),
@@ -81,9 +82,11 @@ class Net:
         import torch
         return C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
 
-    def predict(self, rho, pot_in, guess, cnst: float, stream=None):
-        _check(_net_lib().gpg_net_predict(self._n, int(rho.shape[0]), rho.data_ptr(), pot_in.data_ptr(),
-                                          guess.data_ptr(), cnst, self._s(stream)))
+    def predict(self, rho, pot_in, guess, cnst: float, stream=None, fused: bool = True):
+        """Interior guess; `fused` False runs the per-layer kernels instead."""
+        fn = _net_lib().gpg_net_predict if fused else _net_lib().gpg_net_predict_layers
+        _check(fn(self._n, int(rho.shape[0]), rho.data_ptr(), pot_in.data_ptr(), guess.data_ptr(), cnst,
+                  self._s(stream)))
 
     def gradients(self, rho, pot_in, target, cnst: float, grad=None, loss=None, stream=None):
         _check(_net_lib().gpg_net_gradients(self._n, int(rho.shape[0]), rho.data_ptr(), pot_in.data_ptr(),

@@ -1,0 +1,220 @@
+"""Train and evaluate the learned initial guess for ghost-size-1 SOR.
+
+    python gpu_testbed_poisson-gravity_b200/learned.py train --npatch 1048576 --epochs 2 \
+        --out gpu_testbed_poisson-gravity_b200/lib/learned_init
+    python gpu_testbed_poisson-gravity_b200/learned.py eval  --npatch 65536 \
+        --weights gpu_testbed_poisson-gravity_b200/lib/learned_init
+
+Data: seeded ghost-1 patches (gpg.inputs) with rho0 log-uniform over 4
+decades and power index uniform in [1.5, 2.5].  Targets are the plain SOR's own
+solutions (reference rule from the interpolated start, i.e. converged to the
+FP32 round-off floor) computed by libgpg.  Training and inference run on the
+library's tensor-core kernels (gpg_net_*).  Evaluation solves held-out patches
+(other seeds) from a zero start and from the learned guess to the same
+relative tolerance and reports sweeps, patches/s (the network's inference
+included) and the error against an FP64 solution of the same patches.
+Weights are saved as <out>.bin (float32) with a <out>.json header.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+from gpg.abi import (GPG_INIT_GUESS, GPG_INIT_ZERO, GPG_SOR, GPG_STOP_TOLERANCE,  # noqa: E402
+                     default_params)
+from gpg.inputs import log_uniform, make_patches  # noqa: E402
+
+CNST = float(np.float32(np.float32(4 * np.pi * 1e-5) * np.float32(1.0) * np.float32(1.0)))
+CHUNK = 65536
+# algorithmic FLOPs of one patch's forward pass: 3^3 convolutions 3 -> 32 -> 32
+# -> 32 on the 10^3 cube, 32 -> 1 on the 8^3 interior
+NET_FLOP = 2 * 27 * (1000 * (3 * 32 + 32 * 32 + 32 * 32) + 512 * 32)
+
+
+def dataset(n: int, seed: int, dtype=np.float32):
+    """(rho [n][8]^3, pot_in [n][8]^3) for ghost-1 patches, generated in chunks."""
+    rho = np.empty((n, 8, 8, 8), dtype=dtype)
+    pin = np.empty((n, 8, 8, 8), dtype=dtype)
+    for c0 in range(0, n, CHUNK):
+        m = min(CHUNK, n - c0)
+        s = seed * 1000 + c0 // CHUNK
+        rng = np.random.Generator(np.random.PCG64(s + 7))
+        d = make_patches(m, 1, seed=s, rho0=log_uniform(m, s + 3), index=rng.uniform(1.5, 2.5, m),
+                         dtype=dtype, fluid=False)
+        rho[c0:c0 + m] = d["rho"]
+        pin[c0:c0 + m] = d["pot_in"]
+    return rho, pin
+
+
+def sor_params(real_size: int, init_mode: int, stop_mode: int = GPG_STOP_TOLERANCE, tol: float = 0.02,
+               max_iter: int = 300):
+    return default_params(real_size, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=init_mode, stop_mode=stop_mode,
+                          sor_tolerance=tol, sor_min_iter=1, sor_max_iter=max_iter)
+
+
+def solve(torch, p, rho, pin, guess=None):
+    from gpg.lib import solve_device
+    pot, _, it, rs = solve_device(p, rho, pin, guess=guess)
+    return pot, it, rs
+
+
+def targets(torch, rho, pin):
+    """The plain SOR's own converged solutions: reference rule, interpolated start."""
+    p = default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0)
+    pot, _, _ = solve(torch, p, rho, pin)
+    return pot
+
+
+def save(net, path: str, meta: dict):
+    flat = net.params()
+    flat.tofile(path + ".bin")
+    with open(path + ".json", "w") as f:
+        json.dump(dict(meta, nparams=int(flat.size), dtype="float32",
+                       layers=[[8, 32], [32, 32], [32, 32], [32, 16]],
+                       layout="per layer W[27][cin][cout] then b[cout]"), f, indent=1)
+
+
+def load(net, path: str):
+    flat = np.fromfile(path + ".bin", dtype=np.float32)
+    if flat.size != net.nparams:
+        raise ValueError(f"{path}.bin has {flat.size} parameters, the network {net.nparams}")
+    net.set_params(flat)
+
+
+def train(npatch: int, epochs: int, batch: int, lr: float, seed: int, out: str | None, log=print):
+    import torch
+    from gpg.net import Net
+    dev = torch.device("cuda:0")
+    t0 = time.time()
+    rho_h, pin_h = dataset(npatch, seed)
+    rho, pin = torch.from_numpy(rho_h).to(dev), torch.from_numpy(pin_h).to(dev)
+    del rho_h, pin_h
+    tgt = targets(torch, rho, pin)
+    torch.cuda.synchronize()
+    t_data = time.time() - t0
+    net = Net(max_batch=batch, seed=seed)
+    loss = torch.empty(1, device=dev)
+    nstep = epochs * (npatch // batch)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hist = []
+    s_ev.record()
+    step = 0
+    for ep in range(epochs):
+        perm = torch.randperm(npatch // batch, generator=g)
+        for bi in perm.tolist():
+            sl = slice(bi * batch, (bi + 1) * batch)
+            cur_lr = lr * 0.5 * (1 + np.cos(np.pi * step / max(1, nstep)))   # cosine schedule
+            net.train_step(rho[sl], pin[sl], tgt[sl], CNST, float(cur_lr), loss=loss)
+            step += 1
+            if step % 200 == 0 or step == nstep:
+                hist.append((step, float(loss.item())))
+                log(f"step {step}/{nstep} loss {hist[-1][1]:.4e}")
+    e_ev.record()
+    torch.cuda.synchronize()
+    net.check()
+    ms = s_ev.elapsed_time(e_ev)
+    meta = {"npatch": npatch, "epochs": epochs, "batch": batch, "lr": lr, "seed": seed, "steps": nstep,
+            "train_ms": ms, "ms_per_step": ms / max(1, nstep), "data_s": t_data, "loss_history": hist}
+    if out:
+        save(net, out, meta)
+    return net, meta
+
+
+def _event_ms(torch, fn, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def evaluate(net, npatch: int, seed: int, tol: float = 0.02):
+    """Zero-start plain SOR vs learned-guess SOR to the same relative tolerance."""
+    import torch
+    dev = torch.device("cuda:0")
+    rho_h, pin_h = dataset(npatch, seed)
+    rho, pin = torch.from_numpy(rho_h).to(dev), torch.from_numpy(pin_h).to(dev)
+    p0 = sor_params(4, GPG_INIT_ZERO, tol=tol)
+    pg = sor_params(4, GPG_INIT_GUESS, tol=tol)
+    guess = torch.empty((npatch, 8, 8, 8), device=dev)
+    out = {}
+    ms_plain = _event_ms(torch, lambda: solve(torch, p0, rho, pin))
+    pot0, it0, _ = solve(torch, p0, rho, pin)
+    ms_net = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST))
+    ms_net_layers = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST, fused=False))
+    net.predict(rho, pin, guess, CNST)
+    ms_sor_g = _event_ms(torch, lambda: solve(torch, pg, rho, pin, guess=guess))
+    potg, itg, _ = solve(torch, pg, rho, pin, guess=guess)
+    net.check()
+    # FP64 solution of the same patches: reference rule from the interpolated start
+    p64 = default_params(8, 1, GPG_SOR, gra_acc=0, gra_ghost=0)
+    pot64, _, _ = solve(torch, p64, rho.double(), pin.double())
+    ref = pot64.cpu().numpy().reshape(npatch, -1)
+
+    def err(pot):
+        a = pot.double().cpu().numpy().reshape(npatch, -1)
+        return float((np.abs(a - ref).max(1) / np.abs(ref).max(1)).max())
+
+    def stats(it):
+        a = it.cpu().numpy()
+        return {"mean": float(a.mean()), "p50": float(np.median(a)), "p90": float(np.percentile(a, 90)),
+                "max": int(a.max())}
+
+    out["tolerance"] = f"L1 residual <= {tol} x L1 source norm, Min_Iter 1, Max_Iter 300, FP32"
+    out["plain_zero_start"] = {"sweeps": stats(it0), "ms": ms_plain, "patches_per_s": npatch / ms_plain * 1e3,
+                               "rel_linf_vs_fp64": err(pot0)}
+    out["learned_init"] = {"sweeps": stats(itg), "ms_network": ms_net, "ms_network_per_layer_kernels": ms_net_layers,
+                           "network_tflops": NET_FLOP * npatch / ms_net * 1e-9, "ms_sor": ms_sor_g,
+                           "ms": ms_net + ms_sor_g, "patches_per_s": npatch / (ms_net + ms_sor_g) * 1e3,
+                           "rel_linf_vs_fp64": err(potg)}
+    g = guess.double().cpu().numpy().reshape(npatch, -1)
+    out["learned_init"]["guess_rel_linf_vs_fp64"] = float((np.abs(g - ref).max(1) / np.abs(ref).max(1)).mean())
+    out["speedup_vs_plain"] = ms_plain / (ms_net + ms_sor_g)
+    out["sweep_ratio"] = out["plain_zero_start"]["sweeps"]["mean"] / max(1e-9, out["learned_init"]["sweeps"]["mean"])
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--npatch", type=int, default=1 << 20)
+    t.add_argument("--epochs", type=int, default=2)
+    t.add_argument("--batch", type=int, default=1024)
+    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--out", default=os.path.join(HERE, "lib", "learned_init"))
+    t.add_argument("--eval", type=int, default=65536, help="held-out patches evaluated after training (0: none)")
+    e = sub.add_parser("eval")
+    e.add_argument("--npatch", type=int, default=65536)
+    e.add_argument("--weights", default=os.path.join(HERE, "lib", "learned_init"))
+    e.add_argument("--seed", type=int, default=99)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        net, meta = train(a.npatch, a.epochs, a.batch, a.lr, a.seed, a.out)
+        print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
+        if a.eval:
+            print(json.dumps(evaluate(net, a.eval, 99), indent=1))
+    else:
+        from gpg.net import Net
+        net = Net(max_batch=4096)
+        load(net, a.weights)
+        print(json.dumps(evaluate(net, a.npatch, a.seed), indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

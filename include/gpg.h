@@ -255,9 +255,15 @@ GPG_API int gpg_net_destroy(gpg_net *net);
 GPG_API int gpg_net_param_count(int64_t *count);
 GPG_API int gpg_net_get_params(gpg_net *net, float *host_params);
 GPG_API int gpg_net_set_params(gpg_net *net, const float *host_params);
-/* interior guess [P][8]^3 for GPG_INIT_GUESS (stream-ordered) */
+/* interior guess [P][8]^3 for GPG_INIT_GUESS (stream-ordered): one
+ * persistent kernel runs all four layers with the activations in shared
+ * memory; no size limit from max_batch */
 GPG_API int gpg_net_predict(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in, float *d_guess,
                             double cnst, void *stream);
+/* the same guess through the per-layer kernels of the training pass (chunks
+ * of max_batch patches); identical results, kept for checking */
+GPG_API int gpg_net_predict_layers(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in,
+                                   float *d_guess, double cnst, void *stream);
 /* loss = mean (net / s - target / s)^2 over interior cells and its gradient
  * wrt every parameter (d_grad, same layout as the parameters; may be NULL) */
 GPG_API int gpg_net_gradients(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in,

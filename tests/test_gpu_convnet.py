@@ -100,3 +100,46 @@ def test_training_reduces_loss(torch):
     net.check()
     assert loss.item() < 0.5 * first
     net.close()
+
+
+@pytest.mark.parametrize("npatch", [1, 150, 1000])
+def test_fused_predict_matches_layers(torch, npatch):
+    """The one-kernel forward pass equals the per-layer kernels bit for bit
+    (1 patch; fewer patches than SMs; several patches per CTA, so the weight
+    ring wraps across layers and patches)."""
+    from gpg.inputs import log_uniform
+    from gpg.net import Net
+    rng = np.random.default_rng(npatch)
+    d = make_patches(npatch, 1, seed=40 + npatch, rho0=log_uniform(npatch, 5), index=rng.uniform(1.5, 2.5, npatch),
+                     fluid=False)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    net = Net(max_batch=256, seed=9)
+    p = net.params()
+    p += 0.05 * rng.standard_normal(p.size).astype(np.float32)   # every bias and weight non-trivial
+    net.set_params(p)
+    fused = torch.full((npatch, 8, 8, 8), float("nan"), device="cuda")
+    layers = torch.full((npatch, 8, 8, 8), float("nan"), device="cuda")
+    net.predict(rho, pin, fused, float(CNST))
+    net.predict(rho, pin, layers, float(CNST), fused=False)
+    torch.cuda.synchronize()
+    net.check()
+    assert not torch.isnan(fused).any()
+    assert torch.equal(fused, layers)
+    net.close()
+
+
+def test_learned_guess_reduces_sweeps(torch):
+    """A network trained briefly on the plain SOR's own solutions (ghost 1,
+    rho0 log-uniform, power index in [1.5, 2.5]) starts the SOR closer to the
+    solution: fewer sweeps to the same relative L1 tolerance on held-out
+    patches, at the same error against the FP64 solution."""
+    import learned
+    net, meta = learned.train(npatch=65536, epochs=2, batch=512, lr=2e-3, seed=3, out=None, log=lambda *a: None)
+    assert meta["loss_history"][-1][1] < 0.1 * meta["loss_history"][0][1] or meta["loss_history"][-1][1] < 1e-3
+    r = learned.evaluate(net, 4096, seed=77)
+    plain, guess = r["plain_zero_start"], r["learned_init"]
+    assert guess["sweeps"]["mean"] < 0.85 * plain["sweeps"]["mean"], r
+    assert guess["sweeps"]["p50"] < plain["sweeps"]["p50"], r
+    # both stop at the same residual tolerance: same error scale against FP64
+    assert guess["rel_linf_vs_fp64"] <= 3 * plain["rel_linf_vs_fp64"] + 1e-6, r
+    net.close()
