@@ -2,14 +2,18 @@
 // one persistent kernel: one patch at a time per CTA, its activations resident
 // in shared memory from the interpolated input to the predicted interior.
 //
-// Layout.  A patch's 10^3 solver cube is stored zero-padded to 12^3 "rows"
-// (row = (z+1)*144 + (y+1)*12 + (x+1) for cube cell (x, y, z)); each row holds
-// the cell's channels as 16-byte chunks, chunk c of row r at c*1584*16 + r*16
-// (the no-swizzle K-major core-matrix layout: 8 rows x 16 bytes contiguous;
-// consecutive chunks share their zero end planes, see kChunkRows).
-// Because rows are contiguous, the im2col operand of tap (dz, dy, dx) for a
-// 128-row tile is the same buffer read from a start row shifted by
-// off = 144 dz + 12 dy + dx: the convolution needs no gather at all, only one
+// Layout.  A patch's 10^3 solver cube is stored as rows
+// row = (z+1)*121 + (y+1)*11 + (x+1) for cube cell (x, y, z): lines of 11
+// rows (10 cells and one zero halo column) and planes of 11 lines (10 and one
+// zero halo line), with zero halo planes before and after.  A neighbour one
+// step outside the cube in x (or y) wraps onto the halo column (line) that
+// follows, so one zero slot serves both sides.  Each row holds the cell's
+// channels as 16-byte chunks, chunk c of row r at c*1331*16 + r*16 (the
+// no-swizzle K-major core-matrix layout: 8 rows x 16 bytes contiguous;
+// consecutive chunks share their zero end planes, see kChunkRows).  Because
+// rows are contiguous, the im2col operand of tap (dz, dy, dx) for a 128-row
+// tile is the same buffer read from a start row shifted by
+// off = 121 dz + 11 dy + dx: the convolution needs no gather at all, only one
 // shared-memory descriptor per (tile, tap, K half).  The zero halo supplies the
 // "same" padding; tile rows that are not cube cells produce values that the
 // epilogue discards (their reads stay inside the kernel's shared memory).
@@ -25,7 +29,8 @@
 //     same arithmetic as the SOR) into scratch, s = max |shell|, build the
 //     8-channel input rows; then per layer thread 0 issues tcgen05.mma for
 //     every tile as each unit lands (M=128, N=32 or 16, K=16, BF16 -> FP32 in
-//     TMEM; all 12 tiles of a patch accumulate at once in 384 TMEM columns)
+//     TMEM; all 10 tiles of a patch accumulate at once in 320 TMEM columns,
+//     layer 4's 8 tiles in the next 128)
 //     -- it waits only for weights, never for MMAs; one mbarrier wait per
 //     unit of up to 96 MMAs -- and all 8 warps run the epilogue (tcgen05.ld; bias,
 //     ReLU, BF16) into the other activation buffer; layer 4 writes (y + b) * s
@@ -44,18 +49,21 @@
 namespace gpg {
 namespace net {
 
-constexpr int kPadRows = 1728;          // 12^3
-constexpr int kRowCube = 157;           // padded row of cube cell (0,0,0)
-constexpr int kRowInterior = 314;       // padded row of interior cell (1,1,1)
-constexpr int kTilesCube = 12;          // 128-row tiles over rows 157..1692 (cube rows end at 1570)
-constexpr int kTilesInterior = 9;       // 128-row tiles over rows 314..1465 (interior rows end at 1413)
-// Chunk regions are chained 1584 rows apart: the last z-plane of a chunk
-// (rows 1584..1727, all halo) is the first z-plane of the next (rows 0..143,
-// all halo).  Both are zero for the kernel's life, so sharing them is exact
-// and saves 8 x 144 rows (18 KB) for the weight ring.
-constexpr int kChunkRows = 1584;
+constexpr int kLine = 11;               // rows per y line: 10 cells + 1 shared halo column
+constexpr int kPlane = 121;             // rows per z plane: 10 lines + 1 shared halo line
+constexpr int kRowCube = 133;           // row of cube cell (0,0,0) = 121 + 11 + 1
+constexpr int kRowInterior = 266;       // row of interior cell (1,1,1)
+constexpr int kMaxOffset = 133;         // largest |tap offset|
+constexpr int kTilesCube = 10;          // 128-row tiles over rows 133..1412 (cube rows end at 1330)
+constexpr int kTilesInterior = 8;       // 128-row tiles over rows 266..1289 (interior rows end at 1197)
+constexpr int kColsL4 = kTilesCube * 32;  // layer-4 accumulators follow those of layers 1-3 in TMEM
+// Chunk regions are chained 1331 rows apart: the halo plane after a chunk's
+// last cell plane (rows 1331..1451) is the halo plane before the next chunk's
+// first (rows 0..120).  Both are zero for the kernel's life, so sharing them
+// is exact.
+constexpr int kChunkRows = 11 * kPlane;
 constexpr uint32_t kChunkBytes = kChunkRows * 16u;
-constexpr uint32_t kChainBytes = (8u * kChunkRows + 144u) * 16u;  // buffers A and B, 4 chunks each
+constexpr uint32_t kChainBytes = (8u * kChunkRows + kPlane) * 16u;  // buffers A and B, 4 chunks each
 constexpr int kRing = 3;                // weight ring slots
 constexpr uint32_t kSlotBytes = 8192;   // a unit: up to 4 taps (32 -> 32), 8 tap pairs (layer 1) or 8 taps (layer 4)
 __host__ __device__ constexpr int units_of_layer(int l) { return l == 0 ? 2 : l == 3 ? 4 : 7; }
@@ -67,7 +75,7 @@ constexpr int kInferThreads = kComputeThreads + 32; // + one producer warp for t
 struct InferSmem {
   static constexpr uint32_t buf_a = 0;
   static constexpr uint32_t buf_b = 4 * kChunkBytes;
-  static constexpr uint32_t ring = kChainBytes;
+  static constexpr uint32_t ring = (kChainBytes + 1023u) & ~1023u;
   static constexpr uint32_t bias = ring + kRing * kSlotBytes;  // 32 + 32 + 32 + 16 floats
   static constexpr uint32_t bars = bias + 112 * 4;             // full[4], empty[4], acc
   static constexpr uint32_t tmem_slot = bars + (2 * kRing + 1) * 8;
@@ -76,9 +84,10 @@ struct InferSmem {
   static constexpr uint32_t bytes = flag + 16;
 };
 static_assert(InferSmem::bytes <= 232448, "shared memory per CTA");
-// the farthest descriptor read: buffer B, chunk 3, rows up to 157 + 128*11 + 157 + 127 = 1849
-static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + 157) * 16 <= InferSmem::bytes,
+// the farthest descriptor read: buffer B, chunk 3, rows up to 133 + 128*9 + 133 + 127 = 1545
+static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + kMaxOffset) * 16 <= InferSmem::bytes,
               "shifted tile reads stay inside shared memory");
+static_assert(kColsL4 + kTilesInterior * 16 <= 512, "TMEM columns");
 static_assert(InferSmem::ring % 128 == 0, "ring alignment");
 
 struct InferArgs {
@@ -93,8 +102,9 @@ struct InferArgs {
 };
 
 __host__ __device__ constexpr int tap_offset(int t) {
-  return (t / 9 - 1) * 144 + ((t / 3) % 3 - 1) * 12 + (t % 3 - 1);
+  return (t / 9 - 1) * kPlane + ((t / 3) % 3 - 1) * kLine + (t % 3 - 1);
 }
+static_assert(tap_offset(26) == kMaxOffset && tap_offset(0) == -kMaxOffset, "tap offsets");
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
@@ -179,7 +189,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
   float *s_red = reinterpret_cast<float *>(smem + S::red);
   volatile int *s_abort = reinterpret_cast<volatile int *>(smem + S::flag);
   // scratch for the interpolated cube: buffer B chunk 1, rows 0..249 (the
-  // first 144 are chunk 0's last halo plane); zeroed again before layer 1
+  // first 121 are chunk 0's last halo plane); zeroed again before layer 1
   float *cube = reinterpret_cast<float *>(buf_b + kChunkBytes);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int quarter = warp & 3, half = warp >> 2;  // TMEM lanes 32*quarter.., tiles of parity `half`
@@ -278,7 +288,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
                                         t > 0 ? 1u : 0u);
         } else {
           issue_unit<kTilesInterior, 2, 16>(
-              tmem, tc::smem_desc(a_u32 + uint32_t(kRowInterior + tap_offset(t)) * 16u, CH, 128), 2 * CH / 16,
+              tmem + kColsL4, tc::smem_desc(a_u32 + uint32_t(kRowInterior + tap_offset(t)) * 16u, CH, 128), 2 * CH / 16,
               tc::smem_desc(wsl, 256, 128), 512 / 16, IDESC16, t > 0 ? 1u : 0u);
         }
       }
@@ -310,8 +320,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
       tc::tmem_ld16(ta + 16, v1);
       tc::tmem_wait_ld();
       const int row = kRowCube + 128 * i + 32 * quarter + lane;
-      const int z = row / 144, r2 = row - z * 144, y = r2 / 12, x = r2 - y * 12;
-      if (x >= 1 && x <= 10 && y >= 1 && y <= 10 && z >= 1 && z <= 10) {
+      const int z = row / kPlane, r2 = row - z * kPlane, y = r2 / kLine, x = r2 - y * kLine;
+      if (x >= 1 && y >= 1 && z >= 1 && z <= 10) {  // x, y <= 10 always
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           __align__(16) __nv_bfloat16 o[8];
@@ -358,7 +368,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
       o[2] = __float2bfloat16_rn(shell ? 0.f : 1.f);
 #pragma unroll
       for (int i = 3; i < 8; ++i) o[i] = __float2bfloat16_rn(0.f);
-      const int row = (z + 1) * 144 + (y + 1) * 12 + (x + 1);
+      const int row = (z + 1) * kPlane + (y + 1) * kLine + (x + 1);
       *reinterpret_cast<uint4 *>(buf_b + row * 16) = *reinterpret_cast<const uint4 *>(o);
     }
     compute_sync();
@@ -387,10 +397,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
     wait_acc();
     for (int i = half; i < kTilesInterior; i += 2) {
       const float y4 =
-          __uint_as_float(tmem_ld1(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(i * 16)));
+          __uint_as_float(tmem_ld1(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(kColsL4 + i * 16)));
       tc::tmem_wait_ld();
       const int row = kRowInterior + 128 * i + 32 * quarter + lane;
-      const int z = row / 144, r2 = row - z * 144, y = r2 / 12, x = r2 - y * 12;
+      const int z = row / kPlane, r2 = row - z * kPlane, y = r2 / kLine, x = r2 - y * kLine;
       if (x >= 2 && x <= 9 && y >= 2 && y <= 9 && z >= 2 && z <= 9)
         a.guess[p * 512 + ((z - 2) * 8 + (y - 2)) * 8 + (x - 2)] = (y4 + s_bias[96]) * s;
     }
