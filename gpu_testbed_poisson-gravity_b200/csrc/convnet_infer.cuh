@@ -19,8 +19,8 @@
 // epilogue discards (their reads stay inside the kernel's shared memory).
 //
 // Roles (9 warps):
-//   * producer warp (lane 0): streams the weights in 20 units per patch (up
-//     to 8 KB: 4 taps of a 32 -> 32 layer) through a 3-slot ring with TMA bulk
+//   * producer warp (lane 0): streams the weights in 11 units per patch (up
+//     to 16 KB: 8 taps of a 32 -> 32 layer) through a 3-slot ring with TMA bulk
 //     copies (cp.async.bulk, no multicast), refilling a slot once the MMAs
 //     that read it have completed (tcgen05.commit -> "empty" mbarrier).  The
 //     stream runs across layers and patches, so the next layer's weights land
@@ -32,7 +32,7 @@
 //     TMEM; all 10 tiles of a patch accumulate at once in 320 TMEM columns,
 //     layer 4's 8 tiles in the next 128)
 //     -- it waits only for weights, never for MMAs; one mbarrier wait per
-//     unit of up to 96 MMAs -- and all 8 warps run the epilogue (tcgen05.ld; bias,
+//     unit of up to 160 MMAs -- and all 8 warps run the epilogue (tcgen05.ld; bias,
 //     ReLU, BF16) into the other activation buffer; layer 4 writes (y + b) * s
 //     of output channel 0 on the 8^3 interior straight to the guess array.
 // Every operation and its order matches the per-layer kernels of
@@ -64,11 +64,14 @@ constexpr int kColsL4 = kTilesCube * 32;  // layer-4 accumulators follow those o
 constexpr int kChunkRows = 11 * kPlane;
 constexpr uint32_t kChunkBytes = kChunkRows * 16u;
 constexpr uint32_t kChainBytes = (8u * kChunkRows + kPlane) * 16u;  // buffers A and B, 4 chunks each
+// The issuing thread's wait for a weight unit slows the MMAs that follow it
+// (about 1k cycles per wait measured on B200), so units are large: 16 KB =
+// 8 taps of a 32 -> 32 layer, all 14 tap pairs of layer 1, 16 taps of layer 4.
 constexpr int kRing = 3;                // weight ring slots
-constexpr uint32_t kSlotBytes = 8192;   // a unit: up to 4 taps (32 -> 32), 8 tap pairs (layer 1) or 8 taps (layer 4)
-__host__ __device__ constexpr int units_of_layer(int l) { return l == 0 ? 2 : l == 3 ? 4 : 7; }
-__host__ __device__ constexpr int first_unit(int l) { return l == 0 ? 0 : l == 1 ? 2 : l == 2 ? 9 : 16; }
-constexpr int kUnitsPerPatch = 20;
+constexpr uint32_t kSlotBytes = 16384;
+__host__ __device__ constexpr int units_of_layer(int l) { return l == 0 ? 1 : l == 3 ? 2 : 4; }
+__host__ __device__ constexpr int first_unit(int l) { return l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 5 : 9; }
+constexpr int kUnitsPerPatch = 11;
 constexpr int kComputeThreads = 256;                // 8 warps: input, MMA issue (thread 0), epilogues
 constexpr int kInferThreads = kComputeThreads + 32; // + one producer warp for the weight ring
 
@@ -125,7 +128,7 @@ __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
   return r;
 }
 
-// weight unit u (0..19) of the per-patch stream: its layer, first tap (tap
+// weight unit u (0..10) of the per-patch stream: its layer, first tap (tap
 // pair for layer 1), number of taps and bytes.  A tap's packed operand is
 // 2 KB (32 -> 32) or 1 KB (layer 4, and a tap pair of layer 1).
 struct Unit {
@@ -133,14 +136,16 @@ struct Unit {
   uint32_t tap_bytes;
 };
 __host__ __device__ constexpr Unit unit_info(int u) {
-  return u < 2    ? Unit{0, 8 * u, (14 - 8 * u) < 8 ? (14 - 8 * u) : 8, 1024u}
-         : u < 9  ? Unit{1, 4 * (u - 2), (27 - 4 * (u - 2)) < 4 ? (27 - 4 * (u - 2)) : 4, 2048u}
-         : u < 16 ? Unit{2, 4 * (u - 9), (27 - 4 * (u - 9)) < 4 ? (27 - 4 * (u - 9)) : 4, 2048u}
-                  : Unit{3, 8 * (u - 16), (27 - 8 * (u - 16)) < 8 ? (27 - 8 * (u - 16)) : 8, 1024u};
+  return u < 1   ? Unit{0, 0, 14, 1024u}
+         : u < 5 ? Unit{1, 8 * (u - 1), (27 - 8 * (u - 1)) < 8 ? (27 - 8 * (u - 1)) : 8, 2048u}
+         : u < 9 ? Unit{2, 8 * (u - 5), (27 - 8 * (u - 5)) < 8 ? (27 - 8 * (u - 5)) : 8, 2048u}
+                 : Unit{3, 16 * (u - 9), (27 - 16 * (u - 9)) < 16 ? (27 - 16 * (u - 9)) : 16, 1024u};
 }
-static_assert(unit_info(1).t0 + unit_info(1).ntap == 14 && unit_info(8).t0 + unit_info(8).ntap == 27 &&
-                  unit_info(15).t0 + unit_info(15).ntap == 27 && unit_info(19).t0 + unit_info(19).ntap == 27,
-              "units cover every tap");
+static_assert(unit_info(0).ntap == 14 && unit_info(4).t0 + unit_info(4).ntap == 27 &&
+                  unit_info(8).t0 + unit_info(8).ntap == 27 && unit_info(10).t0 + unit_info(10).ntap == 27 &&
+                  unit_info(3).ntap * unit_info(3).tap_bytes <= kSlotBytes &&
+                  unit_info(9).ntap * unit_info(9).tap_bytes <= kSlotBytes,
+              "units cover every tap and fit a slot");
 __device__ __forceinline__ const unsigned char *unit_src(const InferArgs &a, int u, uint32_t &bytes) {
   const Unit un = unit_info(u);
   bytes = uint32_t(un.ntap) * un.tap_bytes;
