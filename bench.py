@@ -271,7 +271,49 @@ def extra_configs(torch, dev, cpu: bool):
         "workload": "ghost 2-5 x 4096 patches x FP32/FP64, zero interior start, stop at L1 residual <= "
                     "0.02 (FP32) / 5e-11 (FP64) x L1 source norm", "patches_per_s": tot_n / tot_ms * 1e3,
         "per_batch": per}
+    # --- learned initial guess vs plain SOR (ghost 1, FP32) -----------------
+    out["learned_init_sor_g1"] = learned_config(torch)
     return out
+
+
+def learned_config(torch):
+    """The learned-guess configuration: the committed network (trained by
+    learned.py on 2^20 plain-SOR solutions) on 65536 held-out ghost-1 patches
+    (rho0 log-uniform over 4 decades, power index uniform in [1.5, 2.5]):
+    zero-start plain SOR vs network guess + SOR to the same relative L1
+    tolerance, error against the FP64 solution, and the fused network
+    kernel's tensor-core roofline."""
+    import learned
+    from gpg.net import Net
+    if not os.path.exists(learned.DEFAULT_WEIGHTS + ".bin"):
+        return {"unavailable": "no trained weights (run learned.py train)"}
+    net = Net(max_batch=1024)
+    learned.load(net, learned.DEFAULT_WEIGHTS)
+    rec = learned.evaluate(net, 65536, seed=99)
+    net.close()
+    peaks = _measured_peaks()
+    peak = peaks.get("bf16_tflops") if peaks else None
+    ms = rec["learned_init"]["ms_network"]
+    exec_flop = learned.NET_FLOP_EXECUTED * 65536
+    rec["workload"] = ("65536 held-out ghost-1 patches (seed 99), FP32 SOR, network BF16 weights/activations "
+                       "with FP32 accumulation; weights " + os.path.relpath(learned.DEFAULT_WEIGHTS, REPO))
+    rec["network_roofline"] = {
+        "bound": "tensor", "unit": "TFLOP/s",
+        "achieved": rec["learned_init"]["network_tflops"],
+        "achieved_executed": exec_flop / ms * 1e-9,
+        "peak": peak, "peak_kind": "measured bf16 burst" if peak else None,
+        "frac": rec["learned_init"]["network_tflops"] / peak if peak else None,
+        "frac_executed": exec_flop / ms * 1e-9 / peak if peak else None,
+        "flop_per_patch": learned.NET_FLOP, "flop_per_patch_executed": learned.NET_FLOP_EXECUTED}
+    return rec
+
+
+def _measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
 
 
 def main(argv=None) -> int:

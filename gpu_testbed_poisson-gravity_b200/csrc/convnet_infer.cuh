@@ -60,10 +60,12 @@ constexpr int kColsL4 = kTilesCube * 32;  // layer-4 accumulators follow those o
 // Chunk regions are chained 1331 rows apart: the halo plane after a chunk's
 // last cell plane (rows 1331..1451) is the halo plane before the next chunk's
 // first (rows 0..120).  Both are zero for the kernel's life, so sharing them
-// is exact.
+// is exact.  The far corner's neighbour (+1, +1, +1) of cell (9, 9, 9) is row
+// 1463, one plane further (the next chunk's halo line and column): the chain
+// therefore ends with two zero planes after the last chunk, not one.
 constexpr int kChunkRows = 11 * kPlane;
 constexpr uint32_t kChunkBytes = kChunkRows * 16u;
-constexpr uint32_t kChainBytes = (8u * kChunkRows + kPlane) * 16u;  // buffers A and B, 4 chunks each
+constexpr uint32_t kChainBytes = (8u * kChunkRows + 2u * kPlane) * 16u;  // buffers A and B, 4 chunks each
 // The issuing thread's wait for a weight unit slows the MMAs that follow it
 // (about 1k cycles per wait measured on B200), so units are large: 16 KB =
 // 8 taps of a 32 -> 32 layer, all 14 tap pairs of layer 1, 16 taps of layer 4.
@@ -80,7 +82,7 @@ struct InferSmem {
   static constexpr uint32_t buf_b = 4 * kChunkBytes;
   static constexpr uint32_t ring = (kChainBytes + 1023u) & ~1023u;
   static constexpr uint32_t bias = ring + kRing * kSlotBytes;  // 32 + 32 + 32 + 16 floats
-  static constexpr uint32_t bars = bias + 112 * 4;             // full[4], empty[4], acc
+  static constexpr uint32_t bars = bias + 112 * 4;             // full[kRing], empty[kRing], acc
   static constexpr uint32_t tmem_slot = bars + (2 * kRing + 1) * 8;
   static constexpr uint32_t red = tmem_slot + 16;              // 8 floats
   static constexpr uint32_t flag = red + 32;                    // abort flag
@@ -91,6 +93,9 @@ static_assert(InferSmem::bytes <= 232448, "shared memory per CTA");
 static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + kMaxOffset) * 16 <= InferSmem::bytes,
               "shifted tile reads stay inside shared memory");
 static_assert(kColsL4 + kTilesInterior * 16 <= 512, "TMEM columns");
+// every read of a kept (cube) row stays inside the zero-filled chain
+static_assert(InferSmem::buf_b + 3 * kChunkBytes + (10 * kPlane + 10 * kLine + 10 + kMaxOffset + 1) * 16 <= kChainBytes,
+              "kept rows read only the zero-filled chain");
 static_assert(InferSmem::ring % 128 == 0, "ring alignment");
 
 struct InferArgs {
@@ -273,8 +278,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
         *s_abort = 1;
         break;
       }
-      // the copy's completion on the mbarrier orders its bytes before the MMAs
-      // (no tcgen05 fence here: one would drain the tensor pipe every unit)
+      // the wait observed the copy's completion; this fence orders the
+      // asynchronous MMAs below after it (without it they may read the slot
+      // before the copy has landed)
+      tc::fence_after_sync();
       const Unit un = unit_info(u);
       for (int k = 0; k < un.ntap; ++k) {
         const uint32_t wsl = ring_u32 + slot * kSlotBytes + uint32_t(k) * un.tap_bytes;

@@ -1,9 +1,9 @@
 """Train and evaluate the learned initial guess for ghost-size-1 SOR.
 
     python gpu_testbed_poisson-gravity_b200/learned.py train --npatch 1048576 --epochs 2 \
-        --out gpu_testbed_poisson-gravity_b200/lib/learned_init
+        --out gpu_testbed_poisson-gravity_b200/weights/learned_init
     python gpu_testbed_poisson-gravity_b200/learned.py eval  --npatch 65536 \
-        --weights gpu_testbed_poisson-gravity_b200/lib/learned_init
+        --weights gpu_testbed_poisson-gravity_b200/weights/learned_init
 
 Data: seeded ghost-1 patches (gpg.inputs) with rho0 log-uniform over 4
 decades and power index uniform in [1.5, 2.5].  Targets are the plain SOR's own
@@ -13,7 +13,9 @@ library's tensor-core kernels (gpg_net_*).  Evaluation solves held-out patches
 (other seeds) from a zero start and from the learned guess to the same
 relative tolerance and reports sweeps, patches/s (the network's inference
 included) and the error against an FP64 solution of the same patches.
-Weights are saved as <out>.bin (float32) with a <out>.json header.
+Weights are saved as <out>.bin (float32) with a <out>.json header;
+weights/learned_init.* is the checkpoint of the command above (2^20 patches,
+seed 1, 2 epochs of batch 1024, Adam with a cosine learning-rate schedule).
 """
 from __future__ import annotations
 
@@ -34,9 +36,14 @@ from gpg.inputs import log_uniform, make_patches  # noqa: E402
 
 CNST = float(np.float32(np.float32(4 * np.pi * 1e-5) * np.float32(1.0) * np.float32(1.0)))
 CHUNK = 65536
+DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "learned_init")
 # algorithmic FLOPs of one patch's forward pass: 3^3 convolutions 3 -> 32 -> 32
 # -> 32 on the 10^3 cube, 32 -> 1 on the 8^3 interior
 NET_FLOP = 2 * 27 * (1000 * (3 * 32 + 32 * 32 + 32 * 32) + 512 * 32)
+# FLOPs the fused kernel's MMAs execute per patch (M=128 x K=16 tiles): 10 row
+# tiles x 14 tap pairs (N=32) for layer 1, 10 x 27 x 2 K halves (N=32) for
+# layers 2 and 3, 8 x 27 x 2 (N=16) for layer 4
+NET_FLOP_EXECUTED = 2 * 128 * 16 * (32 * (10 * 14 + 2 * 10 * 27 * 2) + 16 * 8 * 27 * 2)
 
 
 def dataset(n: int, seed: int, dtype=np.float32):
@@ -196,11 +203,11 @@ def main(argv=None) -> int:
     t.add_argument("--batch", type=int, default=1024)
     t.add_argument("--lr", type=float, default=2e-3)
     t.add_argument("--seed", type=int, default=1)
-    t.add_argument("--out", default=os.path.join(HERE, "lib", "learned_init"))
+    t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--eval", type=int, default=65536, help="held-out patches evaluated after training (0: none)")
     e = sub.add_parser("eval")
     e.add_argument("--npatch", type=int, default=65536)
-    e.add_argument("--weights", default=os.path.join(HERE, "lib", "learned_init"))
+    e.add_argument("--weights", default=DEFAULT_WEIGHTS)
     e.add_argument("--seed", type=int, default=99)
     a = ap.parse_args(argv)
     if a.cmd == "train":

@@ -143,3 +143,51 @@ def test_learned_guess_reduces_sweeps(torch):
     # both stop at the same residual tolerance: same error scale against FP64
     assert guess["rel_linf_vs_fp64"] <= 3 * plain["rel_linf_vs_fp64"] + 1e-6, r
     net.close()
+
+
+def test_fused_predict_after_other_kernels(torch):
+    """The fused kernel reads no shared memory it has not written: its result
+    is the same right after the per-layer kernels and the SOR solver have left
+    their own data in every SM's shared memory."""
+    from gpg.abi import GPG_SOR, default_params
+    from gpg.lib import solve_device
+    from gpg.net import Net
+    n = 592
+    d = make_patches(n, 1, seed=78, fluid=False)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    net = Net(max_batch=n, seed=6)
+    layers = torch.empty((n, 8, 8, 8), device="cuda")
+    net.predict(rho, pin, layers, float(CNST), fused=False)
+    for other in ("layers", "sor"):
+        if other == "sor":
+            solve_device(default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0), rho, pin)
+        else:
+            net.predict(rho, pin, torch.empty_like(layers), float(CNST), fused=False)
+        fused = torch.full((n, 8, 8, 8), float("nan"), device="cuda")
+        net.predict(rho, pin, fused, float(CNST))
+        torch.cuda.synchronize()
+        net.check()
+        assert torch.equal(fused, layers), other
+    net.close()
+
+
+def test_fused_predict_cold_weights(torch):
+    """The weight ring's copies come from HBM when L2 holds other data: the
+    tensor core must still only read a slot after its copy has landed (L2 is
+    flushed by a 512 MB write before each call)."""
+    from gpg.net import Net
+    n = 1184  # 8 patches per CTA on 148 SMs
+    d = make_patches(n, 1, seed=77, fluid=False)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    net = Net(max_batch=n, seed=4)
+    layers = torch.empty((n, 8, 8, 8), device="cuda")
+    net.predict(rho, pin, layers, float(CNST), fused=False)
+    flush = torch.empty(128 * 2 ** 20, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        flush.fill_(1.0)
+        fused = torch.full((n, 8, 8, 8), float("nan"), device="cuda")
+        net.predict(rho, pin, fused, float(CNST))
+        torch.cuda.synchronize()
+        net.check()
+        assert torch.equal(fused, layers)
+    net.close()
