@@ -194,6 +194,28 @@ def evaluate(net, npatch: int, seed: int, tol: float = 0.02):
     return out
 
 
+def time_predict(npatch: int, reps: int, weights: str | None = DEFAULT_WEIGHTS, per_layer: bool = True):
+    """Device time of the network's forward pass over npatch held-out patches:
+    the one-kernel path and (per_layer) the per-layer kernels, CUDA events."""
+    import torch
+    from gpg.net import Net
+    rho_h, pin_h = dataset(npatch, 99)
+    rho, pin = torch.from_numpy(rho_h).cuda(), torch.from_numpy(pin_h).cuda()
+    net = Net(max_batch=min(npatch, 4096))
+    if weights and os.path.exists(weights + ".bin"):
+        load(net, weights)
+    guess = torch.empty((npatch, 8, 8, 8), device="cuda")
+    out = {"npatch": npatch}
+    for fused in (True, False) if per_layer else (True,):
+        ms = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST, fused=fused), reps)
+        key = "fused" if fused else "per_layer"
+        out[key] = {"ms": ms, "tflops": NET_FLOP * npatch / ms * 1e-9,
+                    "tflops_executed": NET_FLOP_EXECUTED * npatch / ms * 1e-9}
+    net.check()
+    net.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -209,8 +231,14 @@ def main(argv=None) -> int:
     e.add_argument("--npatch", type=int, default=65536)
     e.add_argument("--weights", default=DEFAULT_WEIGHTS)
     e.add_argument("--seed", type=int, default=99)
+    tm = sub.add_parser("time", help="time the network's forward pass")
+    tm.add_argument("--npatch", type=int, default=65536)
+    tm.add_argument("--reps", type=int, default=5)
+    tm.add_argument("--fused-only", action="store_true")
     a = ap.parse_args(argv)
-    if a.cmd == "train":
+    if a.cmd == "time":
+        print(json.dumps(time_predict(a.npatch, a.reps, per_layer=not a.fused_only)))
+    elif a.cmd == "train":
         net, meta = train(a.npatch, a.epochs, a.batch, a.lr, a.seed, a.out)
         print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
         if a.eval:
