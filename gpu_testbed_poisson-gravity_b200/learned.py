@@ -30,8 +30,8 @@ sys.path.insert(0, HERE)
 
 import numpy as np  # noqa: E402
 
-from gpg.abi import (GPG_INIT_GUESS, GPG_INIT_ZERO, GPG_SOR, GPG_STOP_TOLERANCE,  # noqa: E402
-                     default_params)
+from gpg.abi import (GPG_INIT_GUESS, GPG_INIT_INTERP, GPG_INIT_ZERO, GPG_SOR,  # noqa: E402
+                     GPG_STOP_TOLERANCE, default_params)
 from gpg.inputs import log_uniform, make_patches  # noqa: E402
 
 CNST = float(np.float32(np.float32(4 * np.pi * 1e-5) * np.float32(1.0) * np.float32(1.0)))
@@ -149,7 +149,9 @@ def _event_ms(torch, fn, reps=3):
 
 
 def evaluate(net, npatch: int, seed: int, tol: float = 0.02):
-    """Zero-start plain SOR vs learned-guess SOR to the same relative tolerance."""
+    """Zero-start plain SOR vs learned-guess SOR to the same relative tolerance
+    (and the reference's interpolated start beside them), then all three
+    starts under the reference's own stopping rule."""
     import torch
     dev = torch.device("cuda:0")
     rho_h, pin_h = dataset(npatch, seed)
@@ -187,10 +189,28 @@ def evaluate(net, npatch: int, seed: int, tol: float = 0.02):
                            "network_tflops": NET_FLOP * npatch / ms_net * 1e-9, "ms_sor": ms_sor_g,
                            "ms": ms_net + ms_sor_g, "patches_per_s": npatch / (ms_net + ms_sor_g) * 1e3,
                            "rel_linf_vs_fp64": err(potg)}
+    pi = sor_params(4, GPG_INIT_INTERP, tol=tol)
+    ms_interp = _event_ms(torch, lambda: solve(torch, pi, rho, pin))
+    poti, iti, _ = solve(torch, pi, rho, pin)
+    out["plain_interpolated_start"] = {"sweeps": stats(iti), "ms": ms_interp,
+                                       "patches_per_s": npatch / ms_interp * 1e3, "rel_linf_vs_fp64": err(poti)}
     g = guess.double().cpu().numpy().reshape(npatch, -1)
     out["learned_init"]["guess_rel_linf_vs_fp64"] = float((np.abs(g - ref).max(1) / np.abs(ref).max(1)).mean())
     out["speedup_vs_plain"] = ms_plain / (ms_net + ms_sor_g)
     out["sweep_ratio"] = out["plain_zero_start"]["sweeps"]["mean"] / max(1e-9, out["learned_init"]["sweeps"]["mean"])
+    # the reference's own criterion (Min_Iter 10, stop when the L1 residual
+    # grows, Max_Iter 60) from its interpolated start, a zero start and the guess
+    rr = {"criterion": "reference rule: Min_Iter 10, stop at the first growth of the L1 residual, Max_Iter 60, FP32"}
+    for name, mode in (("interpolated_start", GPG_INIT_INTERP), ("zero_start", GPG_INIT_ZERO),
+                       ("learned_start", GPG_INIT_GUESS)):
+        pr = default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=mode)
+        gg = guess if mode == GPG_INIT_GUESS else None
+        ms = _event_ms(torch, lambda: solve(torch, pr, rho, pin, guess=gg))
+        pot, it, _ = solve(torch, pr, rho, pin, guess=gg)
+        tot = ms + (ms_net if mode == GPG_INIT_GUESS else 0.0)
+        rr[name] = {"sweeps": stats(it), "ms": tot, "patches_per_s": npatch / tot * 1e3,
+                    "rel_linf_vs_fp64": err(pot)}
+    out["reference_rule"] = rr
     return out
 
 
