@@ -13,7 +13,10 @@ Reported (one JSON line from rank 0):
              CUDA events on the launching stream, max over ranks)
   e2e        the same through the reference-shaped host API (pinned host
              buffers, H2D + solve + D2H per step; host clock around a full sync)
-  roofline   dominant kernel: compulsory HBM bytes per launch / mean launch time
+  roofline   dominant kernel: compulsory HBM bytes per launch / mean launch time;
+             roofline.onchip: its shared-memory wavefronts per launch (measured
+             sweeps x 3 loads + 1 store per cell update) / launch time, against
+             one wavefront per cycle per SM at the sampled clock
   cpu_baseline  the reference's own CPU code (oracle/_ref, all host threads) on
              a bounded sample of the same workload
 `--impl reference` runs only the reference CPU path (rank 0) and prints its line.
@@ -484,6 +487,23 @@ def main(argv=None) -> int:
     except OSError:
         pass
 
+    # on-chip bound of the same kernel: every cell update is 3 shared loads + 1
+    # shared store; a warp-wide access of 4-byte (8-byte) values is 1 (2)
+    # shared-memory wavefronts; the pipe serves one wavefront per cycle per SM
+    clocks = clk.summary()
+    sm_mhz = float(clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0))
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    g = pk.ghost
+    cell_updates = float(iters[k].astype(np.float64).sum()) * (6 + 2 * g) ** 3
+    wavefronts = cell_updates * 4 * (pk.real_size * 32 // 128) / 32
+    onchip_peak = nsm * sm_mhz * 1e6
+    onchip = {"resource": "shared-memory pipe", "unit": "wavefronts/s",
+              "achieved": wavefronts / (launch_ms / 1e3), "peak": onchip_peak,
+              "frac": wavefronts / (launch_ms / 1e3) / onchip_peak,
+              "algorithmic_wavefronts_per_launch": wavefronts,
+              "model": "measured sweeps x RHO_NXT^3 cell updates x (3 loads + 1 store); 1 wavefront/cycle/SM "
+                       f"at the sampled {sm_mhz:.0f} MHz x {nsm} SMs"}
+
     line = {
         "metric": METRIC, "value": value, "unit": "patches/s", "n_gpus": world, "steps": a.steps,
         "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -492,7 +512,8 @@ def main(argv=None) -> int:
                                "Min 10 / Max 60|100), ghost 2-5 x 4096 patches, FP32+FP64, Poisson only",
                    "global_batch": world * patches_step, "patches_per_gpu": patches_step,
                    "l2": f"step inputs {step_inputs / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
-                   "parallelism": f"patch shards x{world}", "learned_init": "not built"},
+                   "parallelism": f"patch shards x{world}",
+                   "learned_init": "extra.learned_init_sor_g1 (ghost 1, 65536 held-out patches)"},
         "gpu_launches": len(batches) * a.steps,
         "per_batch_ms": {f"f{8 * p.real_size}_g{p.ghost}": float(per_kernel[:, i].mean())
                          for i, (p, _) in enumerate(batches)},
@@ -500,9 +521,10 @@ def main(argv=None) -> int:
         "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
-                     "launch_ms": launch_ms, "peak_source": "measured" if peaks else "fallback"},
+                     "launch_ms": launch_ms, "peak_source": "measured" if peaks else "fallback",
+                     "onchip": onchip},
         "e2e": e2e,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if rank == 0 and not a.no_cpu_baseline and world == 1:
         v, cores, kind, sample = reference_cpu(batches, budget_s=20.0)
