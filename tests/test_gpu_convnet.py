@@ -191,3 +191,31 @@ def test_fused_predict_cold_weights(torch):
         net.check()
         assert torch.equal(fused, layers)
     net.close()
+
+
+def test_net_rejects_bad_input(torch):
+    """Invalid sizes and NULL arrays come back as status codes with a message,
+    never as a launch; zero patches is a no-op."""
+    import ctypes as C
+    from gpg.lib import GpgError
+    from gpg.net import Net, _net_lib
+    lib = _net_lib()
+    bad = C.c_void_p()
+    assert lib.gpg_net_create(C.byref(bad), 0, 1, 0) != 0
+    assert b"max_batch" in lib.gpg_net_last_error()
+    net = Net(max_batch=4, seed=2)
+    assert lib.gpg_net_predict(net._n, 3, None, None, None, 1.0, None) != 0
+    assert b"NULL" in lib.gpg_net_last_error()
+    assert lib.gpg_net_predict(net._n, -1, None, None, None, 1.0, None) != 0
+    assert lib.gpg_net_predict(net._n, 0, None, None, None, 1.0, None) == 0
+    d = make_patches(8, 1, seed=3, fluid=False)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    with pytest.raises(GpgError):
+        net.train_step(rho, pin, torch.zeros((8, 8, 8, 8), device="cuda"), float(CNST), 1e-3)   # 8 > max_batch
+    assert lib.gpg_net_predict(None, 1, None, None, None, 1.0, None) != 0
+    guess = torch.empty((8, 8, 8, 8), device="cuda")
+    net.predict(rho, pin, guess, float(CNST))   # predict has no max_batch limit
+    torch.cuda.synchronize()
+    net.check()
+    assert torch.isfinite(guess).all()
+    net.close()
