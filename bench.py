@@ -349,7 +349,8 @@ def main(argv=None) -> int:
             vals.append(v)
         v = float(np.median(vals))
         line = {"metric": METRIC, "value": v, "unit": "patches/s", "n_gpus": a.gpus, "steps": a.steps,
-                "warmup": a.warmup, "higher_is_better": True, "impl": "reference",
+                "warmup": a.warmup, "ms_per_step": NPATCH * len(batches) / v * 1e3, "scaling": "weak",
+                "higher_is_better": True, "impl": "reference",
                 "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": "plain SOR, reference rule, ghost 2-5 x 4096 patches, FP32+FP64",
                            "global_batch": len(batches) * NPATCH},
