@@ -615,14 +615,26 @@ extern "C" int gpg_net_gradients(gpg_net *n, int npatch, const float *d_rho, con
   return GPG_OK;
 }
 
-extern "C" int gpg_net_train_step(gpg_net *n, int npatch, const float *d_rho, const float *d_pot_in,
-                                  const float *d_target, double cnst, float lr, float *d_loss, void *stream) {
-  if (int rc = gpg_net_gradients(n, npatch, d_rho, d_pot_in, d_target, cnst, nullptr, d_loss, stream)) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+namespace {
+// one Adam step (beta 0.9 / 0.999, eps 1e-8) with gradient `grad`, then the
+// BF16 operands are repacked from the updated FP32 masters
+int adam_step(gpg_net *n, const float *grad, float lr, cudaStream_t s) {
   n->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - std::pow(b1, float(n->step)), c2 = 1.f - std::pow(b2, float(n->step));
-  adam_kernel<<<128, 256, 0, s>>>(n->params, n->adam_m, n->adam_v, n->grad, kParams, lr, b1, b2, 1e-8f, c1, c2);
+  adam_kernel<<<128, 256, 0, s>>>(n->params, n->adam_m, n->adam_v, grad, kParams, lr, b1, b2, 1e-8f, c1, c2);
   NET_CUDA(cudaGetLastError());
   return repack(n, s);
+}
+}  // namespace
+
+extern "C" int gpg_net_train_step(gpg_net *n, int npatch, const float *d_rho, const float *d_pot_in,
+                                  const float *d_target, double cnst, float lr, float *d_loss, void *stream) {
+  if (int rc = gpg_net_gradients(n, npatch, d_rho, d_pot_in, d_target, cnst, nullptr, d_loss, stream)) return rc;
+  return adam_step(n, n->grad, lr, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gpg_net_apply_gradient(gpg_net *n, const float *d_grad, float lr, void *stream) {
+  if (!n || !d_grad) return nfail(GPG_ERR_INVALID, "NULL argument");
+  return adam_step(n, d_grad, lr, static_cast<cudaStream_t>(stream));
 }

@@ -24,6 +24,7 @@ def _net_lib():
             "gpg_net_predict_layers": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp]),
             "gpg_net_gradients": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp]),
             "gpg_net_train_step": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, C.c_float, vp, vp]),
+            "gpg_net_apply_gradient": (C.c_int, [vp, vp, C.c_float, vp]),
             "gpg_net_check": (C.c_int, [vp]),
             "gpg_net_last_error": (C.c_char_p, []),
         }
@@ -98,6 +99,12 @@ class Net:
         _check(_net_lib().gpg_net_train_step(self._n, int(rho.shape[0]), rho.data_ptr(), pot_in.data_ptr(),
                                              target.data_ptr(), cnst, lr,
                                              None if loss is None else loss.data_ptr(), self._s(stream)))
+
+    def apply_gradient(self, grad, lr: float, stream=None):
+        """Adam step with `grad` (a CUDA float32 tensor of nparams values)."""
+        if grad.numel() != self.nparams or not grad.is_cuda or grad.dtype.itemsize != 4 or not grad.is_contiguous():
+            raise ValueError(f"grad must be a contiguous CUDA float32 tensor of {self.nparams} values")
+        _check(_net_lib().gpg_net_apply_gradient(self._n, grad.data_ptr(), lr, self._s(stream)))
 
     def check(self):
         _check(_net_lib().gpg_net_check(self._n))

@@ -95,3 +95,17 @@ def scatter_solve_gather(arrays: dict, solve, group=None, src: int = 0) -> dict 
     for k in names:
         dist.send(torch.from_numpy(np.ascontiguousarray(out[k])), dst=src, group=group)
     return None
+
+
+def allreduce_mean_(t, group=None):
+    """In-place mean of tensor `t` over the ranks of `group` (the gradient
+    exchange of data-parallel training: every rank ends with the same
+    average).  A no-op without an initialised process group."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return t
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    w = dist.get_world_size(group)
+    if w > 1:
+        t.div_(w)
+    return t

@@ -46,19 +46,36 @@ NET_FLOP = 2 * 27 * (1000 * (3 * 32 + 32 * 32 + 32 * 32) + 512 * 32)
 NET_FLOP_EXECUTED = 2 * 128 * 16 * (32 * (10 * 14 + 2 * 10 * 27 * 2) + 16 * 8 * 27 * 2)
 
 
-def dataset(n: int, seed: int, dtype=np.float32):
-    """(rho [n][8]^3, pot_in [n][8]^3) for ghost-1 patches, generated in chunks."""
-    rho = np.empty((n, 8, 8, 8), dtype=dtype)
-    pin = np.empty((n, 8, 8, 8), dtype=dtype)
-    for c0 in range(0, n, CHUNK):
+def dataset(n: int, seed: int, dtype=np.float32, first: int = 0, stop: int | None = None):
+    """(rho, pot_in) [..][8]^3 of ghost-1 patches first..stop of an n-patch set,
+    generated in chunks of CHUNK patches, each from its own seeds; a range
+    that starts on a chunk boundary (a data-parallel shard) gets exactly the
+    patches the whole set has there."""
+    stop = n if stop is None else stop
+    if first % CHUNK or not 0 <= first <= stop <= n:
+        raise ValueError("shard must start on a chunk boundary and lie inside the set")
+    rho = np.empty((stop - first, 8, 8, 8), dtype=dtype)
+    pin = np.empty((stop - first, 8, 8, 8), dtype=dtype)
+    for c0 in range(first, stop, CHUNK):
         m = min(CHUNK, n - c0)
         s = seed * 1000 + c0 // CHUNK
         rng = np.random.Generator(np.random.PCG64(s + 7))
         d = make_patches(m, 1, seed=s, rho0=log_uniform(m, s + 3), index=rng.uniform(1.5, 2.5, m),
                          dtype=dtype, fluid=False)
-        rho[c0:c0 + m] = d["rho"]
-        pin[c0:c0 + m] = d["pot_in"]
+        k = min(m, stop - c0)
+        rho[c0 - first:c0 - first + k] = d["rho"][:k]
+        pin[c0 - first:c0 - first + k] = d["pot_in"][:k]
     return rho, pin
+
+
+def shard(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Rank's [first, stop) of an n-patch training set, whole chunks per rank."""
+    from gpg.shard import shard_bounds
+    nchunk = (n + CHUNK - 1) // CHUNK
+    if world > nchunk:
+        raise ValueError(f"{world} ranks for {nchunk} chunks of {CHUNK} patches")
+    lo, hi = shard_bounds(nchunk, world)[rank]
+    return lo * CHUNK, min(hi * CHUNK, n)
 
 
 def sor_params(real_size: int, init_mode: int, stop_mode: int = GPG_STOP_TOLERANCE, tol: float = 0.02,
@@ -97,41 +114,74 @@ def load(net, path: str):
 
 
 def train(npatch: int, epochs: int, batch: int, lr: float, seed: int, out: str | None, log=print):
+    """Train on npatch patches with global batch `batch`.  Under torchrun
+    (RANK / WORLD_SIZE set) this is data-parallel over NCCL: every rank builds
+    its own chunk shard and the same initial network, computes the gradient of
+    its batch / world patches, the gradients are averaged with an all-reduce
+    and every rank applies the same Adam step; rank 0 saves the checkpoint.
+    One process without a process group runs gpg_net_train_step directly."""
     import torch
+    import torch.distributed as dist
     from gpg.net import Net
-    dev = torch.device("cuda:0")
+    from gpg.shard import allreduce_mean_
+    distributed = "RANK" in os.environ and "WORLD_SIZE" in os.environ
+    rank, world = (int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])) if distributed else (0, 1)
+    if distributed and not dist.is_initialized():
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if batch % world:
+        raise ValueError(f"global batch {batch} is not a multiple of {world} ranks")
+    lb = batch // world
     t0 = time.time()
-    rho_h, pin_h = dataset(npatch, seed)
+    first, stop = shard(npatch, rank, world)
+    rho_h, pin_h = dataset(npatch, seed, first=first, stop=stop)
     rho, pin = torch.from_numpy(rho_h).to(dev), torch.from_numpy(pin_h).to(dev)
     del rho_h, pin_h
     tgt = targets(torch, rho, pin)
     torch.cuda.synchronize()
     t_data = time.time() - t0
-    net = Net(max_batch=batch, seed=seed)
+    nb = (stop - first) // lb
+    if distributed:  # every rank takes the same number of steps
+        t = torch.tensor([nb], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        nb = int(t.item())
+    net = Net(max_batch=lb, seed=seed)
     loss = torch.empty(1, device=dev)
-    nstep = epochs * (npatch // batch)
-    g = torch.Generator(device="cpu").manual_seed(seed)
+    grad = torch.empty(net.nparams, device=dev) if distributed else None
+    nstep = epochs * nb
+    g = torch.Generator(device="cpu").manual_seed(seed + 7919 * rank)
     s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     hist = []
     s_ev.record()
     step = 0
     for ep in range(epochs):
-        perm = torch.randperm(npatch // batch, generator=g)
+        perm = torch.randperm(nb, generator=g)
         for bi in perm.tolist():
-            sl = slice(bi * batch, (bi + 1) * batch)
-            cur_lr = lr * 0.5 * (1 + np.cos(np.pi * step / max(1, nstep)))   # cosine schedule
-            net.train_step(rho[sl], pin[sl], tgt[sl], CNST, float(cur_lr), loss=loss)
+            sl = slice(bi * lb, (bi + 1) * lb)
+            cur_lr = float(lr * 0.5 * (1 + np.cos(np.pi * step / max(1, nstep))))   # cosine schedule
+            if distributed:
+                net.gradients(rho[sl], pin[sl], tgt[sl], CNST, grad=grad, loss=loss)
+                allreduce_mean_(grad)
+                net.apply_gradient(grad, cur_lr)
+            else:
+                net.train_step(rho[sl], pin[sl], tgt[sl], CNST, cur_lr, loss=loss)
             step += 1
             if step % 200 == 0 or step == nstep:
+                if distributed:
+                    allreduce_mean_(loss)
                 hist.append((step, float(loss.item())))
-                log(f"step {step}/{nstep} loss {hist[-1][1]:.4e}")
+                if rank == 0:
+                    log(f"step {step}/{nstep} loss {hist[-1][1]:.4e}")
     e_ev.record()
     torch.cuda.synchronize()
     net.check()
     ms = s_ev.elapsed_time(e_ev)
     meta = {"npatch": npatch, "epochs": epochs, "batch": batch, "lr": lr, "seed": seed, "steps": nstep,
-            "train_ms": ms, "ms_per_step": ms / max(1, nstep), "data_s": t_data, "loss_history": hist}
-    if out:
+            "ranks": world, "train_ms": ms, "ms_per_step": ms / max(1, nstep), "data_s": t_data,
+            "loss_history": hist}
+    if out and rank == 0:
         save(net, out, meta)
     return net, meta
 
@@ -260,9 +310,14 @@ def main(argv=None) -> int:
         print(json.dumps(time_predict(a.npatch, a.reps, per_layer=not a.fused_only)))
     elif a.cmd == "train":
         net, meta = train(a.npatch, a.epochs, a.batch, a.lr, a.seed, a.out)
-        print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
-        if a.eval:
-            print(json.dumps(evaluate(net, a.eval, 99), indent=1))
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
+            if a.eval:
+                print(json.dumps(evaluate(net, a.eval, 99), indent=1))
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.barrier()
+            dist.destroy_process_group()
     else:
         from gpg.net import Net
         net = Net(max_batch=4096)

@@ -271,6 +271,11 @@ GPG_API int gpg_net_gradients(gpg_net *net, int npatch, const float *d_rho, cons
 /* gradients + one Adam step (beta 0.9 / 0.999, eps 1e-8) */
 GPG_API int gpg_net_train_step(gpg_net *net, int npatch, const float *d_rho, const float *d_pot_in,
                                const float *d_target, double cnst, float lr, float *d_loss, void *stream);
+/* one Adam step with a caller-supplied gradient [param_count] on the device
+ * (stream-ordered): data-parallel training computes per-rank gradients with
+ * gpg_net_gradients, averages them across ranks (an all-reduce), and applies
+ * the average here on every rank; gradients + this call = gpg_net_train_step */
+GPG_API int gpg_net_apply_gradient(gpg_net *net, const float *d_grad, float lr, void *stream);
 /* GPG_ERR_CUDA when a tensor-core wait timed out in an earlier call */
 GPG_API int gpg_net_check(gpg_net *net);
 GPG_API const char *gpg_net_last_error(void);

@@ -219,3 +219,50 @@ def test_net_rejects_bad_input(torch):
     net.check()
     assert torch.isfinite(guess).all()
     net.close()
+
+
+def test_gradient_then_apply_equals_train_step(torch):
+    """gpg_net_gradients + gpg_net_apply_gradient (the data-parallel split,
+    with the all-reduce in between) reproduces gpg_net_train_step bit for bit."""
+    from gpg.net import Net
+    d = make_patches(32, 1, seed=12, fluid=False)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    tgt = (pin.mean() * (1 + 0.05 * torch.randn((32, 8, 8, 8), device="cuda",
+                                                generator=torch.Generator(device="cuda").manual_seed(1)))).contiguous()
+    a, b = Net(max_batch=32, seed=8), Net(max_batch=32, seed=8)
+    grad = torch.empty(a.nparams, device="cuda")
+    for it in range(3):
+        a.train_step(rho, pin, tgt, float(CNST), 1e-3)
+        b.gradients(rho, pin, tgt, float(CNST), grad=grad)
+        b.apply_gradient(grad, 1e-3)
+    torch.cuda.synchronize()
+    a.check()
+    b.check()
+    assert np.array_equal(a.params(), b.params())
+    with pytest.raises(ValueError):
+        b.apply_gradient(grad[:10], 1e-3)
+    a.close()
+    b.close()
+
+
+def test_data_parallel_training_under_torchrun(torch, tmp_path):
+    """learned.py train under torchrun (NCCL process group, one rank here: the
+    all-reduce runs, over a world of one) saves the same weights as the
+    single-process run of the same configuration."""
+    import os
+    import subprocess
+    import sys
+    import learned
+    script = os.path.join(os.path.dirname(learned.__file__), "learned.py")
+    args = ["train", "--npatch", "65536", "--epochs", "1", "--batch", "2048", "--eval", "0"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r1 = subprocess.run([sys.executable, script] + args + ["--out", str(tmp_path / "single")], env=env,
+                        capture_output=True, text=True, timeout=600)
+    assert r1.returncode == 0, r1.stderr[-2000:]
+    r2 = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "1",
+                         "--master-addr", "127.0.0.1", "--master-port", "29531", script] + args +
+                        ["--out", str(tmp_path / "dp")], env=env, capture_output=True, text=True, timeout=600)
+    assert r2.returncode == 0, r2.stderr[-2000:]
+    w1 = np.fromfile(str(tmp_path / "single.bin"), dtype=np.float32)
+    w2 = np.fromfile(str(tmp_path / "dp.bin"), dtype=np.float32)
+    assert w1.size == w2.size and np.array_equal(w1, w2)

@@ -83,3 +83,62 @@ def test_scatter_solve_gather_gloo_world2():
         pr.join(timeout=120)
     assert all(pr.exitcode == 0 for pr in procs)
     assert q.get(timeout=5) is True
+
+
+def _mean_worker(rank, world, port, q):
+    import datetime
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "gpu_testbed_poisson-gravity_b200"))
+    import torch
+    import torch.distributed as dist
+    from gpg.shard import allreduce_mean_
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    g = torch.arange(5, dtype=torch.float32) * (rank + 1)      # rank-dependent "gradient"
+    allreduce_mean_(g)
+    q.put((rank, g.tolist()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gradient_mean_gloo_world2():
+    """The gradient exchange of data-parallel training: every rank ends with
+    the same mean of the ranks' gradients."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mean_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    want = [1.5 * i for i in range(5)]
+    assert got[0] == want and got[1] == want
+
+
+def test_training_shards_cover_the_set():
+    """Rank shards of the learned guess's training set are whole chunks that
+    cover it once, and a shard's patches are the whole set's patches there."""
+    import learned
+    C = learned.CHUNK
+    for n in (C, 3 * C + 5, 16 * C):
+        for w in (1, 2, 3):
+            if w > (n + C - 1) // C:
+                continue
+            b = [learned.shard(n, r, w) for r in range(w)]
+            assert b[0][0] == 0 and b[-1][1] == n
+            assert all(b[i][1] == b[i + 1][0] for i in range(w - 1))
+            assert all(lo % C == 0 for lo, _ in b)
+    with pytest.raises(ValueError):
+        learned.shard(C, 0, 2)
+    n = C + 40
+    full_rho, full_pin = learned.dataset(n, 5)
+    part_rho, part_pin = learned.dataset(n, 5, first=C, stop=n)
+    assert np.array_equal(part_rho, full_rho[C:]) and np.array_equal(part_pin, full_pin[C:])
+    with pytest.raises(ValueError):
+        learned.dataset(n, 5, first=7, stop=n)
