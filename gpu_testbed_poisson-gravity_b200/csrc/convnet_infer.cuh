@@ -18,21 +18,21 @@
 // "same" padding; tile rows that are not cube cells produce values that the
 // epilogue discards (their reads stay inside the kernel's shared memory).
 //
-// Roles (9 warps):
-//   * producer warp (lane 0): streams the weights in 11 units per patch (up
-//     to 16 KB: 8 taps of a 32 -> 32 layer) through a 3-slot ring with TMA bulk
+// Roles (17 warps):
+//   * producer warp (lane 0): streams the weights in 6 units per patch (up
+//     to 28 KB: 14 taps of a 32 -> 32 layer) through a 2-slot ring with TMA bulk
 //     copies (cp.async.bulk, no multicast), refilling a slot once the MMAs
 //     that read it have completed (tcgen05.commit -> "empty" mbarrier).  The
 //     stream runs across layers and patches, so the next layer's weights land
 //     during the epilogue;
-//   * 8 compute warps, per patch: interpolate the coarse potential (CQUAD,
+//   * 16 compute warps, per patch: interpolate the coarse potential (CQUAD,
 //     same arithmetic as the SOR) into scratch, s = max |shell|, build the
 //     8-channel input rows; then per layer thread 0 issues tcgen05.mma for
 //     every tile as each unit lands (M=128, N=32 or 16, K=16, BF16 -> FP32 in
 //     TMEM; all 10 tiles of a patch accumulate at once in 320 TMEM columns,
 //     layer 4's 8 tiles in the next 128)
 //     -- it waits only for weights, never for MMAs; one mbarrier wait per
-//     unit of up to 160 MMAs -- and all 8 warps run the epilogue (tcgen05.ld; bias,
+//     unit of up to 280 MMAs -- and all 16 warps run the epilogue (tcgen05.ld; bias,
 //     ReLU, BF16) into the other activation buffer; layer 4 writes (y + b) * s
 //     of output channel 0 on the 8^3 interior straight to the guess array.
 // Every operation and its order matches the per-layer kernels of
@@ -67,31 +67,38 @@ constexpr int kChunkRows = 11 * kPlane;
 constexpr uint32_t kChunkBytes = kChunkRows * 16u;
 constexpr uint32_t kChainBytes = (8u * kChunkRows + 2u * kPlane) * 16u;  // buffers A and B, 4 chunks each
 // The issuing thread's wait for a weight unit slows the MMAs that follow it
-// (about 1k cycles per wait measured on B200), so units are large: 16 KB =
-// 8 taps of a 32 -> 32 layer, all 14 tap pairs of layer 1, 16 taps of layer 4.
-constexpr int kRing = 3;                // weight ring slots
-constexpr uint32_t kSlotBytes = 16384;
-__host__ __device__ constexpr int units_of_layer(int l) { return l == 0 ? 1 : l == 3 ? 2 : 4; }
-__host__ __device__ constexpr int first_unit(int l) { return l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 5 : 9; }
-constexpr int kUnitsPerPatch = 11;
-constexpr int kComputeThreads = 256;                // 8 warps: input, MMA issue (thread 0), epilogues
+// (about 1k cycles per wait measured on B200), so units are as large as the
+// shared memory left by the activations allows: two 28 KB slots, 6 units per
+// patch (layer 1's 14 tap pairs; 14 + 13 taps of each 32 -> 32 layer; layer
+// 4's 27 taps).  While the tensor core works through one slot (>= 260 MMAs)
+// the producer refills the other.
+constexpr int kRing = 2;                // weight ring slots
+constexpr uint32_t kSlotBytes = 14 * 2048;
+__host__ __device__ constexpr int units_of_layer(int l) { return l == 0 || l == 3 ? 1 : 2; }
+__host__ __device__ constexpr int first_unit(int l) { return l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 3 : 5; }
+constexpr int kUnitsPerPatch = 6;
+constexpr int kComputeThreads = 512;                // 16 warps: input, MMA issue (thread 0), epilogues
 constexpr int kInferThreads = kComputeThreads + 32; // + one producer warp for the weight ring
+constexpr int kTileGroups = kComputeThreads / 128;  // warps sharing one TMEM lane quarter
 
 struct InferSmem {
   static constexpr uint32_t buf_a = 0;
   static constexpr uint32_t buf_b = 4 * kChunkBytes;
-  static constexpr uint32_t ring = (kChainBytes + 1023u) & ~1023u;
-  static constexpr uint32_t bias = ring + kRing * kSlotBytes;  // 32 + 32 + 32 + 16 floats
+  // control data in the gap between the activation chain and the ring (no
+  // descriptor read reaches it)
+  static constexpr uint32_t bias = kChainBytes;                 // 32 + 32 + 32 + 16 floats
   static constexpr uint32_t bars = bias + 112 * 4;             // full[kRing], empty[kRing], acc
   static constexpr uint32_t tmem_slot = bars + (2 * kRing + 1) * 8;
-  static constexpr uint32_t red = tmem_slot + 16;              // 8 floats
-  static constexpr uint32_t flag = red + 32;                    // abort flag
-  static constexpr uint32_t bytes = flag + 16;
+  static constexpr uint32_t red = tmem_slot + 16;              // one float per compute warp
+  static constexpr uint32_t flag = red + 4 * (kComputeThreads / 32);  // abort flag
+  static constexpr uint32_t ring = (flag + 16 + 1023u) & ~1023u;
+  static constexpr uint32_t bytes = ring + kRing * kSlotBytes;
 };
 static_assert(InferSmem::bytes <= 232448, "shared memory per CTA");
+static_assert(InferSmem::bars % 8 == 0, "mbarrier alignment");
 // the farthest descriptor read: buffer B, chunk 3, rows up to 133 + 128*9 + 133 + 127 = 1545
-static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + kMaxOffset) * 16 <= InferSmem::bytes,
-              "shifted tile reads stay inside shared memory");
+static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + kMaxOffset) * 16 <= kChainBytes,
+              "shifted tile reads stay inside the activation chain");
 static_assert(kColsL4 + kTilesInterior * 16 <= 512, "TMEM columns");
 // every read of a kept (cube) row stays inside the zero-filled chain
 static_assert(InferSmem::buf_b + 3 * kChunkBytes + (10 * kPlane + 10 * kLine + 10 + kMaxOffset + 1) * 16 <= kChainBytes,
@@ -133,7 +140,7 @@ __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
   return r;
 }
 
-// weight unit u (0..10) of the per-patch stream: its layer, first tap (tap
+// weight unit u (0..5) of the per-patch stream: its layer, first tap (tap
 // pair for layer 1), number of taps and bytes.  A tap's packed operand is
 // 2 KB (32 -> 32) or 1 KB (layer 4, and a tap pair of layer 1).
 struct Unit {
@@ -142,14 +149,15 @@ struct Unit {
 };
 __host__ __device__ constexpr Unit unit_info(int u) {
   return u < 1   ? Unit{0, 0, 14, 1024u}
-         : u < 5 ? Unit{1, 8 * (u - 1), (27 - 8 * (u - 1)) < 8 ? (27 - 8 * (u - 1)) : 8, 2048u}
-         : u < 9 ? Unit{2, 8 * (u - 5), (27 - 8 * (u - 5)) < 8 ? (27 - 8 * (u - 5)) : 8, 2048u}
-                 : Unit{3, 16 * (u - 9), (27 - 16 * (u - 9)) < 16 ? (27 - 16 * (u - 9)) : 16, 1024u};
+         : u < 3 ? Unit{1, 14 * (u - 1), u == 1 ? 14 : 13, 2048u}
+         : u < 5 ? Unit{2, 14 * (u - 3), u == 3 ? 14 : 13, 2048u}
+                 : Unit{3, 0, 27, 1024u};
 }
-static_assert(unit_info(0).ntap == 14 && unit_info(4).t0 + unit_info(4).ntap == 27 &&
-                  unit_info(8).t0 + unit_info(8).ntap == 27 && unit_info(10).t0 + unit_info(10).ntap == 27 &&
-                  unit_info(3).ntap * unit_info(3).tap_bytes <= kSlotBytes &&
-                  unit_info(9).ntap * unit_info(9).tap_bytes <= kSlotBytes,
+static_assert(unit_info(0).ntap == 14 && unit_info(2).t0 + unit_info(2).ntap == 27 &&
+                  unit_info(4).t0 + unit_info(4).ntap == 27 && unit_info(5).ntap == 27 &&
+                  unit_info(1).ntap * unit_info(1).tap_bytes <= kSlotBytes &&
+                  unit_info(5).ntap * unit_info(5).tap_bytes <= kSlotBytes &&
+                  first_unit(3) + units_of_layer(3) == kUnitsPerPatch,
               "units cover every tap and fit a slot");
 __device__ __forceinline__ const unsigned char *unit_src(const InferArgs &a, int u, uint32_t &bytes) {
   const Unit un = unit_info(u);
@@ -202,7 +210,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
   // first 121 are chunk 0's last halo plane); zeroed again before layer 1
   float *cube = reinterpret_cast<float *>(buf_b + kChunkBytes);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;  // TMEM lanes 32*quarter.., tiles of parity `half`
+  const int quarter = warp & 3, group = warp >> 2;  // TMEM lanes 32*quarter.., tiles group, group+4, ...
 
   // both activation buffers start at zero; the epilogues write cube rows only,
   // so the halo rows stay zero for the kernel's life
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
 
   // epilogue of layers 1-3: bias + ReLU -> bf16 rows of `dst`
   auto epilogue_relu = [&](unsigned char *dst, const float *bias) {
-    for (int i = half; i < kTilesCube; i += 2) {
+    for (int i = group; i < kTilesCube; i += kTileGroups) {
       float v[32];
       float (&v0)[16] = *reinterpret_cast<float(*)[16]>(v);
       float (&v1)[16] = *reinterpret_cast<float(*)[16]>(v + 16);
@@ -407,7 +415,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
       __syncwarp();
     }
     wait_acc();
-    for (int i = half; i < kTilesInterior; i += 2) {
+    for (int i = group; i < kTilesInterior; i += kTileGroups) {
       const float y4 =
           __uint_as_float(tmem_ld1(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(kColsL4 + i * 16)));
       tc::tmem_wait_ld();
