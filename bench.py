@@ -87,7 +87,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
             time.sleep(0.3)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -135,7 +135,7 @@ def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0):
     kind = "reference" if all(ref_available("sor", p.ghost, 1, "f32" if p.real_size == 4 else "f64")
                               for p, _ in batches) else "port"
     cores = nthreads or (oracle_lib().oracle_max_threads())
-    # per batch sample: first n patches (multiple of 8), sized from a probe run
+    # per batch sample: n patches spread over the batch, sized from a probe run
     total_t, total_p, desc = 0.0, 0, []
     per_batch = budget_s / len(batches)
     for p, d in batches:
@@ -158,8 +158,11 @@ def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0):
 
 def _run_cpu(kind, p, d, n, nthreads):
     from oracle.oracle import run_oracle, run_reference
-    rho = np.ascontiguousarray(d["rho"][:n])
-    pin = np.ascontiguousarray(d["pot_in"][:n])
+    # n patches spread evenly over the batch (patch positions cover the box in
+    # order, so a prefix would be one corner of it)
+    idx = np.linspace(0, len(d["rho"]) - 1, n).round().astype(np.int64)
+    rho = np.ascontiguousarray(d["rho"][idx])
+    pin = np.ascontiguousarray(d["pot_in"][idx])
     if kind == "reference":
         q = p.copy(gra_acc=0)
         run_reference(q, rho, pin.copy(), nthreads=nthreads)
@@ -322,7 +325,7 @@ def _measured_peaks():
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -342,10 +345,11 @@ def main(argv=None) -> int:
         batches = workload(0)
         t_all = []
         for _ in range(a.warmup):
-            reference_cpu(batches, budget_s=2.0)
+            reference_cpu(batches, budget_s=min(2.0, 10.0 / max(1, a.warmup)))
         vals = []
         for _ in range(a.steps):
-            v, cores, kind, sample = reference_cpu(batches, budget_s=8.0)
+            # bounded CPU sample per step; the whole run stays near a minute
+            v, cores, kind, sample = reference_cpu(batches, budget_s=max(0.8, min(8.0, 48.0 / max(1, a.steps))))
             vals.append(v)
         v = float(np.median(vals))
         line = {"metric": METRIC, "value": v, "unit": "patches/s", "n_gpus": a.gpus, "steps": a.steps,
