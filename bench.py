@@ -30,6 +30,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -79,7 +80,7 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"gpg_bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -171,7 +172,7 @@ def _run_cpu(kind, p, d, n, nthreads):
 
 
 # ---------------------------------------------------------------------------
-# other BASELINE configurations, measured beside the headline (not the bench value)
+# the other configurations of the path, measured beside the headline (not the bench value)
 # ---------------------------------------------------------------------------
 def _event_ms(torch, fn, reps=5, warm=3):
     for _ in range(warm):
@@ -330,7 +331,7 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the other BASELINE configurations")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other configurations (MG, mixed batch, learned guess)")
     ap.add_argument("--only", default=None,
                     help="comma list of batches to run (e.g. f64_g5); profiling cases, not a bench line")
     a = ap.parse_args(argv)
