@@ -128,10 +128,11 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference CPU path
 # ---------------------------------------------------------------------------
-def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0):
+def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0, keep: dict | None = None):
     """Time the reference's CPU_PoissonGravitySolver (oracle/_ref; the C port
     of oracle/ when the reference objects are absent) on a bounded sample of
-    every batch.  Returns (patches/s, cores, kind, sample description)."""
+    every batch.  Returns (patches/s, cores, kind, sample description); `keep`
+    receives {batch index: (patch indices, potential)} of the timed runs."""
     from oracle.oracle import oracle_lib, ref_available, run_oracle, run_reference
     kind = "reference" if all(ref_available("sor", p.ghost, 1, "f32" if p.real_size == 4 else "f64")
                               for p, _ in batches) else "port"
@@ -149,8 +150,10 @@ def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0):
                 break
             n = min(len(d["rho"]), n * 4)
         t0 = time.perf_counter()
-        _run_cpu(kind, p, d, n, nthreads)
+        res = _run_cpu(kind, p, d, n, nthreads)
         dt = time.perf_counter() - t0
+        if keep is not None:
+            keep[len(desc)] = res
         total_t += dt
         total_p += n
         desc.append(f"g{p.ghost}/f{8 * p.real_size}:{n}")
@@ -166,9 +169,39 @@ def _run_cpu(kind, p, d, n, nthreads):
     pin = np.ascontiguousarray(d["pot_in"][idx])
     if kind == "reference":
         q = p.copy(gra_acc=0)
-        run_reference(q, rho, pin.copy(), nthreads=nthreads)
+        pot = run_reference(q, rho, pin.copy(), nthreads=nthreads)[0]
     else:
-        run_oracle(p, rho, pin, accum_f64=False, nthreads=nthreads)
+        pot = run_oracle(p, rho, pin, accum_f64=False, nthreads=nthreads)[0]
+    return idx, pot
+
+
+def rel_linf(a, b) -> float:
+    """max over patches of ||a - b||_inf / ||b||_inf"""
+    a = np.asarray(a, dtype=np.float64).reshape(len(a), -1)
+    b = np.asarray(b, dtype=np.float64).reshape(len(b), -1)
+    return float((np.abs(a - b).max(1) / np.maximum(np.abs(b).max(1), 1e-300)).max())
+
+
+def headline_errors(torch, batches, dev_in, keep: dict) -> dict:
+    """Relative L-infinity error of every batch's potential against the
+    reference CPU solver (on the patches its timed sample solved) and, for the
+    FP32 batches, against the FP64 solution of the same inputs (the library's
+    FP64 path, which equals the FP64 CPU restatement bit for bit)."""
+    from gpg.lib import solve_device
+    out = {}
+    for k, ((p, _), t) in enumerate(zip(batches, dev_in)):
+        gpu = t["pot_out"].cpu().numpy()
+        rec = {}
+        if k in keep:
+            idx, ref = keep[k]
+            rec["vs_reference_cpu"] = rel_linf(gpu[idx], ref)
+            rec["patches_vs_reference_cpu"] = int(len(idx))
+        if p.real_size == 4:
+            p64 = default_params(8, p.ghost, GPG_SOR, gra_acc=0)
+            pot64 = solve_device(p64, t["rho"].double(), t["pot_in"].double())[0]
+            rec["vs_fp64"] = rel_linf(gpu, pot64.cpu().numpy())
+        out[f"f{8 * p.real_size}_g{p.ghost}"] = rec
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -209,13 +242,24 @@ def extra_configs(torch, dev, cpu: bool):
     ms = _event_ms(torch, lambda: solve_device(p, t["rho"], t["pot_in"], pot_out=pot, flu=flu, iters=it, resid=rs))
     rec = {"workload": "MG V-cycle, ghost 3, FP32 (FP64 error norm), 5-point gravity, 16384 patches",
            "patches_per_s": n / ms * 1e3, "ms": ms, "cycles_mean": float(it.float().mean())}
+    # errors of one fresh solve (the timed calls updated the fluid repeatedly)
+    flu1 = t["flu"].clone()
+    solve_device(p, t["rho"], t["pot_in"], pot_out=pot, flu=flu1, iters=it, resid=rs)
+    gpot, gflu = pot.cpu().numpy(), flu1.cpu().numpy()
+    p64 = default_params(8, 3, 2, gra_ghost=2, p5_gradient=1)
+    pot64, flu64, _, _ = solve_device(p64, t["rho"].double(), t["pot_in"].double(), flu=t["flu"].double())
+    rec["errors"] = {"pot_vs_fp64": rel_linf(gpot, pot64.cpu().numpy()),
+                     "flu_vs_fp64": rel_linf(gflu, flu64.cpu().numpy())}
     if cpu:
         from oracle.oracle import ref_available, run_reference
         if ref_available("mg", 3, 2, "f32"):
             m = 2048
             t0 = time.perf_counter()
-            run_reference(p, np.ascontiguousarray(d["rho"][:m]), d["pot_in"][:m].copy(), flu=d["flu"][:m].copy())
+            rpot, rflu, _ = run_reference(p, np.ascontiguousarray(d["rho"][:m]), d["pot_in"][:m].copy(),
+                                          flu=d["flu"][:m].copy())
             rec["cpu_reference_patches_per_s"] = m / (time.perf_counter() - t0)
+            rec["errors"]["pot_vs_reference_cpu"] = rel_linf(gpot[:m], rpot)
+            rec["errors"]["flu_vs_reference_cpu"] = rel_linf(gflu[:m], rflu)
     out["mg_gravity_g3_f32_16384"] = rec
     # --- mixed batch ---------------------------------------------------------
     N = 65536
@@ -533,8 +577,10 @@ def main(argv=None) -> int:
         "clocks": clocks,
     }
     if rank == 0 and not a.no_cpu_baseline and world == 1:
-        v, cores, kind, sample = reference_cpu(batches, budget_s=20.0)
+        keep = {}
+        v, cores, kind, sample = reference_cpu(batches, budget_s=20.0, keep=keep)
         line["cpu_baseline"] = {"value": v, "unit": "patches/s", "cores": cores, "kind": kind, "sample": sample}
+        line["errors"] = headline_errors(torch, batches, dev_in, keep)
     if rank == 0 and not a.no_extra and not a.only and world == 1:
         line["extra"] = extra_configs(torch, dev, cpu=not a.no_cpu_baseline)
     if rank == 0:
