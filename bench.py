@@ -551,7 +551,9 @@ def main(argv=None) -> int:
               "achieved": wavefronts / (launch_ms / 1e3), "peak": onchip_peak,
               "frac": wavefronts / (launch_ms / 1e3) / onchip_peak,
               "algorithmic_wavefronts_per_launch": wavefronts,
-              "model": "measured sweeps x RHO_NXT^3 cell updates x (3 loads + 1 store); 1 wavefront/cycle/SM "
+              "achieved_gbs": wavefronts * 128 / (launch_ms / 1e3) / 1e9, "peak_gbs": onchip_peak * 128 / 1e9,
+              "model": "measured sweeps x RHO_NXT^3 cell updates x (3 loads + 1 store); 1 wavefront "
+                       "(128 B)/cycle/SM "
                        f"at the sampled {sm_mhz:.0f} MHz x {nsm} SMs"}
 
     line = {
