@@ -178,3 +178,23 @@ def test_empty_and_invalid(torch_cuda):
     bad = default_params(4, 2, GPG_SOR, p5_gradient=1)  # needs gra_ghost 2
     with pytest.raises(GpgError):
         gpu_run(torch, bad, d)
+
+
+@pytest.mark.parametrize("rs", [4, 8])
+def test_full_batch_matches_reference_cpu(torch_cuda, rs):
+    """At the benchmark's size (4096 patches, ghost 5, reference parameters and
+    stopping rule, Poisson only) the potential equals the reference's own CPU
+    solver; the per-patch tolerance is the stated 1e-5 (FP32) / 1e-12 (FP64)
+    relative L-infinity, and with the same sweep counts the bits agree."""
+    from oracle.oracle import ref_available, run_reference
+    prec = "f32" if rs == 4 else "f64"
+    if not ref_available("sor", 5, 1, prec):
+        pytest.skip("reference CPU objects not built")
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(4096, 5, seed=1005, dtype=dt, fluid=False)   # the benchmark's ghost-5 batch
+    p = default_params(rs, 5, GPG_SOR, gra_acc=0)
+    gp = gpu_run(torch_cuda, p, d)[0]
+    rp = run_reference(p, np.ascontiguousarray(d["rho"]), d["pot_in"].copy())[0]
+    assert rel_linf(gp, rp) <= TOL[rs]
+    same = np.all(gp.reshape(4096, -1) == rp.reshape(4096, -1), axis=1)
+    assert same.mean() >= 0.99
