@@ -259,8 +259,12 @@ def test_data_parallel_training_under_torchrun(torch, tmp_path):
     r1 = subprocess.run([sys.executable, script] + args + ["--out", str(tmp_path / "single")], env=env,
                         capture_output=True, text=True, timeout=600)
     assert r1.returncode == 0, r1.stderr[-2000:]
+    import socket
+    with socket.socket() as so:   # a free rendezvous port
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
     r2 = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "1",
-                         "--master-addr", "127.0.0.1", "--master-port", "29531", script] + args +
+                         "--master-addr", "127.0.0.1", "--master-port", str(port), script] + args +
                         ["--out", str(tmp_path / "dp")], env=env, capture_output=True, text=True, timeout=600)
     assert r2.returncode == 0, r2.stderr[-2000:]
     w1 = np.fromfile(str(tmp_path / "single.bin"), dtype=np.float32)
