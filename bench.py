@@ -590,6 +590,11 @@ def main(argv=None) -> int:
         "per_batch_ms": {f"f{8 * p.real_size}_g{p.ghost}": float(per_kernel[:, i].mean())
                          for i, (p, _) in enumerate(batches)},
         "mean_iters": {f"f{8 * p.real_size}_g{p.ghost}": float(it.mean()) for (p, _), it in zip(batches, iters)},
+        "onchip_frac_per_batch": {
+            f"f{8 * p.real_size}_g{p.ghost}":
+                float(it.astype(np.float64).sum()) * (6 + 2 * p.ghost) ** 3 * 4 * (p.real_size * 32 // 128) / 32
+                / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
+            for i, ((p, _), it) in enumerate(zip(batches, iters))},
         "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
