@@ -406,6 +406,7 @@ struct gpg_context {
   std::vector<cudaStream_t> streams;
   gpg_params shape{};
   int64_t cap = 0;  // patches the buffers hold
+  bool allocated = false;  // gpg_mem_allocate succeeded (cap may be 0)
   int64_t n_rho = 0, n_pin = 0, n_pout = 0, n_flu = 0;
   void *d_rho = nullptr, *d_pin = nullptr, *d_pout = nullptr, *d_flu = nullptr;
   int32_t *d_iters = nullptr;
@@ -471,6 +472,8 @@ static void release_buffers(gpg_context *c) {
   c->h_iters = nullptr;
   c->h_resid = nullptr;
   c->cap = 0;
+  c->allocated = false;
+  c->last_npatch = 0;  // gpg_last_iterations has nothing to read any more
 }
 
 extern "C" int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int npatch_group, void **h_rho,
@@ -478,7 +481,7 @@ extern "C" int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int n
   if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
   if (int rc = gpg_validate_params(shape)) return rc;
   if (npatch_group < 0) return fail(GPG_ERR_INVALID, "npatch_group %d", npatch_group);
-  if (ctx->cap) return fail(GPG_ERR_STATE, "buffers already allocated (call gpg_mem_free first)");
+  if (ctx->allocated) return fail(GPG_ERR_STATE, "buffers already allocated (call gpg_mem_free first)");
   GPG_CUDA(cudaSetDevice(ctx->device));
   ctx->shape = *shape;
   ctx->cap = 8 * (int64_t)npatch_group;
@@ -513,6 +516,7 @@ extern "C" int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int n
   }
   for (int k = 0; k < 4; ++k)
     if (outs[k]) *outs[k] = pinned[k];
+  ctx->allocated = true;
   return GPG_OK;
 }
 
@@ -546,9 +550,12 @@ extern "C" int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_r
                                                void *h_flu, int npatch_group, const gpg_params *p, int nstream) {
   if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
   if (int rc = gpg_validate_params(p)) return rc;
-  if (!ctx->cap && npatch_group > 0) return fail(GPG_ERR_STATE, "no buffers (call gpg_mem_allocate first)");
-  if (p->real_size != ctx->shape.real_size || p->ghost != ctx->shape.ghost || p->gra_ghost != ctx->shape.gra_ghost)
+  if (!ctx->allocated) {
+    if (npatch_group > 0) return fail(GPG_ERR_STATE, "no buffers (call gpg_mem_allocate first)");
+  } else if (p->real_size != ctx->shape.real_size || p->ghost != ctx->shape.ghost ||
+             p->gra_ghost != ctx->shape.gra_ghost) {
     return fail(GPG_ERR_INVALID, "parameters do not match the allocated shape");
+  }
   if (p->poisson && p->init_mode == GPG_INIT_GUESS)
     return fail(GPG_ERR_UNSUPPORTED, "GPG_INIT_GUESS needs the device API");
   const int64_t npatch = 8 * (int64_t)npatch_group;

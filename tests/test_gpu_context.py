@@ -74,3 +74,20 @@ def test_context_errors(torch):
             ctx.asyn_solve(p.copy(ghost=3), 2)  # shape differs from the allocation
         with pytest.raises(GpgError):
             ctx.allocate(p, 2)                # double allocation
+    with Context(0, nstream=1) as ctx:
+        ctx.allocate(p, 0)                    # empty allocation still counts as allocated
+        with pytest.raises(GpgError) as e:
+            ctx.allocate(p, 1)
+        assert e.value.status == 6
+        ctx.free()
+        bufs = ctx.allocate(p, 1)             # allowed again after gpg_mem_free
+        assert bufs[0].shape[0] == 8
+        for b in bufs:
+            b[...] = 0
+        ctx.asyn_solve(p, 1)
+        ctx.synchronize()
+        it, _ = ctx.iterations(8)
+        assert it.shape == (8,)
+        ctx.free()
+        with pytest.raises(GpgError):
+            ctx.iterations(8)                 # buffers released: nothing left to read
