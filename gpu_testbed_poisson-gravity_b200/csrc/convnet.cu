@@ -253,6 +253,9 @@ int set_attr_once(F *fn, size_t bytes, std::once_flag &once, cudaError_t &err) {
   return GPG_OK;
 }
 
+// blocks of the bias-gradient and loss kernels = partial sums they leave
+constexpr int kPartials = 148;
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -370,7 +373,7 @@ int conv_weight_grad(gpg_net *n, int l, const __nv_bfloat16 *x, const __nv_bfloa
     rc = launch_wgrad<32, 16>(a, grid, s);
   }
   if (rc) return rc;
-  const int nb = 148;
+  const int nb = kPartials;
   if (kCout[l] == 32)
     bias_grad_kernel<32><<<nb, 256, 0, s>>>(g, n->bpart, M);
   else
@@ -398,7 +401,7 @@ int gradients(gpg_net *n, int64_t npatch, const float *rho, const float *pot_in,
               float *loss, cudaStream_t s) {
   const int64_t M = npatch * kCells;
   if (int rc = forward_all(n, npatch, rho, pot_in, cnst, s)) return rc;
-  const int nlp = 148;
+  const int nlp = kPartials;
   loss_grad_kernel<<<nlp, 256, 0, s>>>(n->y4, target, n->scale, n->g4, n->loss_part, npatch);
   NET_CUDA(cudaGetLastError());
   // layer 4, then 3, 2, 1
@@ -486,8 +489,8 @@ extern "C" int gpg_net_create(gpg_net **out, int max_batch, uint64_t seed, int d
   al((void **)&n->cube, size_t(max_batch) * kCells * 4);
   al((void **)&n->scale, size_t(max_batch) * 4);
   al((void **)&n->wpart, size_t(max_grid) * wrows * 32 * 4);
-  al((void **)&n->bpart, size_t(148) * 32 * 4);
-  al((void **)&n->loss_part, 148 * 8);
+  al((void **)&n->bpart, size_t(kPartials) * 32 * 4);
+  al((void **)&n->loss_part, kPartials * 8);
   al((void **)&n->err, 4);
   if (e != cudaSuccess) {
     free_net(n);
