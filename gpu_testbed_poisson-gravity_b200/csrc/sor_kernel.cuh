@@ -45,8 +45,11 @@ template <typename T, int G>
 struct SorCfg {
   using g = Geo<G>;
   static constexpr bool F64 = sizeof(T) == 8;
-  // lanes per row (R >= HALF; R > HALF pads rows so wavefronts hold whole rows)
-  static constexpr int R = (G == 1) ? 4 : (G == 2 ? 5 : 8);
+  // lanes per row (R >= HALF; R > HALF pads rows so wavefronts hold whole rows;
+  // FP64 ghost 2 pads its 5-pair rows to 6 lanes, which with P = 11 makes every
+  // 64-bit access of a half-warp conflict-free -- with 5 lanes per row the
+  // first half-warp of each class took two wavefronts per access)
+  static constexpr int R = (G == 1) ? 4 : (G == 2 ? (F64 ? 6 : 5) : 8);
   // row pitch (words), bank-conflict-free choice per configuration
   static constexpr int P = (G == 1) ? (F64 ? 6 : 12) : (G == 2 ? (F64 ? 11 : 13) : (G == 3 ? (F64 ? 11 : 12) : 12));
   static constexpr int ROWS_PER_CLASS = g::M / 2;
