@@ -12,7 +12,9 @@ Reported (one JSON line from rank 0):
   value      patches/s over the whole job, inputs resident in HBM (device timing,
              CUDA events on the launching stream, max over ranks)
   e2e        the same through the reference-shaped host API (pinned host
-             buffers, H2D + solve + D2H per step; host clock around a full sync)
+             buffers, H2D + solve + D2H per step; host clock around a full sync;
+             batches pipelined across steps, lockstep_value with a full sync
+             after every step)
   roofline   dominant kernel: compulsory HBM bytes per launch / mean launch time;
              roofline.onchip: its shared-memory wavefronts per launch (measured
              sweeps x 3 loads + 1 store per cell update) / launch time, against
@@ -501,24 +503,33 @@ def main(argv=None) -> int:
             rho[...] = d["rho"]
             pin[...] = d["pot_in"]
             ctxs.append(c)
-        for _ in range(2):
-            for (p, _), c in zip(batches, ctxs):
-                c.asyn_solve(p, NPATCH // 8)
+        def e2e_run(steps, pipelined):
+            # pipelined: a batch waits only for its own previous results (on the
+            # host) before its next inputs go out, so the copy engines never
+            # drain between steps; lockstep: every step ends with a full sync
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                for (p, _), c in zip(batches, ctxs):
+                    if pipelined:
+                        c.synchronize()
+                    c.asyn_solve(p, NPATCH // 8)
+                if not pipelined:
+                    for c in ctxs:
+                        c.synchronize()
             for c in ctxs:
                 c.synchronize()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            for (p, _), c in zip(batches, ctxs):
-                c.asyn_solve(p, NPATCH // 8)
-            for c in ctxs:
-                c.synchronize()
-        barrier()
-        e2e_s = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
+            barrier()
+            el = time.perf_counter() - t0
+            if world > 1:
+                t = torch.tensor([el], device=dev)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                el = float(t.item())
+            return el
+
+        e2e_run(2, False)
+        e2e_s = e2e_run(a.steps, True)
+        lock_s = e2e_run(a.steps, False)
         h2d = step_inputs
         d2h = sum(NPATCH * (patch_sizes(p)["pot_out"] * p.real_size + 4 + 8) for p, _ in batches)
         # host link: pinned -> device copy bandwidth, the bound of this leg
@@ -530,6 +541,9 @@ def main(argv=None) -> int:
         e2e = {"value": world * patches_step * a.steps / e2e_s, "unit": "patches/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "timing": "host clock around full device sync",
+               "pipelining": "each batch's previous results are on the host before its next inputs are "
+                             "issued; no global sync between steps",
+               "lockstep_value": world * patches_step * a.steps / lock_s,
                "h2d_link_gbs": link_gbs,
                "h2d_bound_patches_per_s": world * patches_step / (h2d / (link_gbs * 1e9))}
         for c in ctxs:
