@@ -83,8 +83,8 @@ constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4};
 constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true};
 int g_sor_variant[2][6] = {
     // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
-    {0, 1, 1, 1, 0, 1},   // float
-    {0, 4, 0, 0, 0, 1},   // double
+    {0, 1, 0, 0, 0, 0},   // float
+    {0, 1, 0, 1, 1, 0},   // double
 };
 std::once_flag g_tune_once;
 

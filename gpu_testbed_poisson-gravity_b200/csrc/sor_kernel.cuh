@@ -57,6 +57,12 @@ struct SorCfg {
   static constexpr int TEAM = ((2 * CW0 + 31) / 32) * 32;
   static constexpr int CW = TEAM / 2;  // lanes per row-parity class
   static constexpr int NWARP = TEAM / 32;
+  // every warp holds lanes of one row-parity class only, so the side of a
+  // lane's colour-c cell (left / right of its pair) is warp-uniform and the
+  // passes are compiled per side.  FP64 only: there it frees registers (FP64
+  // g5 phased 202 -> 166, a third team per SM) and each x select is two
+  // instructions; the FP32 kernels measured 9-15 % slower at g4/g5 with it.
+  static constexpr bool UNIFORM = F64 && CW % 32 == 0;
   static constexpr int PP = g::N * P;  // plane pitch
   static constexpr int CUBE = 2 * g::N * PP;
   static_assert(R >= g::HALF && P >= g::HALF + 2, "row layout");
@@ -78,15 +84,22 @@ struct SorSmem {
 // One pass of colour p over every height of the lane's pair: reads the other
 // colour (registers + 3 shared loads per cell), updates v[p][*] in registers,
 // then publishes them.  SUM: accumulate |R| into acc4 (skipped for sweeps
-// whose residual total the stopping rule never looks at).
-template <typename T, int G, bool PHASED, int p, bool SUM>
+// whose residual total the stopping rule never looks at).  SIDE: -1 = the
+// lane's side (left_even) is a run-time value; 0 / 1 = it is known at compile
+// time (warp-uniform layouts dispatch once per pass), which turns the x
+// operand selects and the outside-neighbour address into constants.
+template <typename T, int G, bool PHASED, int p, bool SUM, int SIDE>
 __device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2][Geo<G>::M], T *s_cube,
-                                         int own, int xo_even, int xo_odd, bool left_even, T omega_6,
+                                         int own, int xo_even_rt, int xo_odd_rt, bool left_even_rt, T omega_6,
                                          double (&acc4)[4]) {
   using C = SorCfg<T, G>;
   constexpr int N = Geo<G>::N, M = Geo<G>::M, P = C::P, PP = C::PP;
   const T *nb = s_cube + (1 - p) * N * PP;  // planes of the other colour
   T *mine = s_cube + p * N * PP;
+  const bool left_even = SIDE < 0 ? left_even_rt : SIDE == 1;
+  // outside x neighbour: slot own-1 for a left cell, own+1 for a right one
+  const int xo_even = SIDE < 0 ? xo_even_rt : (SIDE == 1 ? own - 1 : own + 1);
+  const int xo_odd = SIDE < 0 ? xo_odd_rt : (SIDE == 1 ? own + 1 : own - 1);
   // all reads of the pass come from the other colour's planes and all writes
   // go to this colour's planes, so the M updates are independent; the stores
   // follow all of them
@@ -133,6 +146,20 @@ __device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2
   }
 #pragma unroll
   for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
+}
+
+template <typename T, int G, bool PHASED, int p, bool SUM>
+__device__ __forceinline__ void sor_pass_any(T (&v)[2][Geo<G>::N], const T (&crho)[2][Geo<G>::M], T *s_cube,
+                                             int own, int xo_even, int xo_odd, bool left_even, T omega_6,
+                                             double (&acc4)[4]) {
+  if constexpr (SorCfg<T, G>::UNIFORM) {
+    if (left_even)  // warp-uniform branch
+      sor_pass<T, G, PHASED, p, SUM, 1>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    else
+      sor_pass<T, G, PHASED, p, SUM, 0>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+  } else {
+    sor_pass<T, G, PHASED, p, SUM, -1>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+  }
 }
 
 // Solve patch P_ with the team `team` (thread `tid` of TEAM) whose shared
@@ -230,15 +257,15 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
     // deterministic and identical for a patch solved alone or in a batch
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
     if (!need) {
-      if (active) sor_pass<T, G, PHASED, 0, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      if (active) sor_pass_any<T, G, PHASED, 0, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
       team_sync<TEAM>(team);
-      if (active) sor_pass<T, G, PHASED, 1, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      if (active) sor_pass_any<T, G, PHASED, 1, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
       team_sync<TEAM>(team);
       continue;
     }
-    if (active) sor_pass<T, G, PHASED, 0, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    if (active) sor_pass_any<T, G, PHASED, 0, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
     team_sync<TEAM>(team);
-    if (active) sor_pass<T, G, PHASED, 1, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    if (active) sor_pass_any<T, G, PHASED, 1, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
     double acc = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
     acc = warp_sum(acc);
     if constexpr (NWARP > 1) {
