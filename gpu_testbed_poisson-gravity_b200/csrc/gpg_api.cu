@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -81,7 +82,8 @@ int ensure_smem(KernelFn *fn, size_t bytes, AttrOnce &st) {
 constexpr int kSorVariants = 6;
 constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4};
 constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true};
-int g_sor_variant[2][6] = {
+// atomic: gpg_set_sor_variant may run on one host thread while another launches
+std::atomic<int> g_sor_variant[2][6] = {
     // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
     {0, 1, 0, 0, 0, 0},   // float
     {0, 1, 0, 1, 1, 0},   // double
@@ -109,7 +111,8 @@ void load_tune_file() {
   int g, v;
   while (std::fscanf(f, "%7s %d %d", prec, &g, &v) == 3) {
     const int t = std::strcmp(prec, "f64") == 0 ? 1 : (std::strcmp(prec, "f32") == 0 ? 0 : -1);
-    if (t >= 0 && g >= 1 && g <= 5 && v >= 0 && v < kSorVariants) g_sor_variant[t][g] = v;
+    if (t >= 0 && g >= 1 && g <= 5 && v >= 0 && v < kSorVariants)
+      g_sor_variant[t][g].store(v, std::memory_order_relaxed);
   }
   std::fclose(f);
 }
@@ -149,7 +152,7 @@ int prepare_sor_v() {
 template <typename T, int G>
 int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   std::call_once(g_tune_once, load_tune_file);
-  switch (g_sor_variant[sizeof(T) == 8][G]) {
+  switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
     case 0: return launch_sor_v<T, G, 1, false>(a, s);
     case 1: return launch_sor_v<T, G, 1, true>(a, s);
     case 2: return launch_sor_v<T, G, 2, false>(a, s);
@@ -162,7 +165,7 @@ int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
 template <typename T, int G>
 int prepare_sor() {
   std::call_once(g_tune_once, load_tune_file);
-  switch (g_sor_variant[sizeof(T) == 8][G]) {
+  switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
     case 0: return prepare_sor_v<T, G, 1, false>();
     case 1: return prepare_sor_v<T, G, 1, true>();
     case 2: return prepare_sor_v<T, G, 2, false>();
@@ -664,7 +667,7 @@ extern "C" int gpg_set_sor_variant(int real_size, int ghost, int variant) {
   std::call_once(g_tune_once, load_tune_file);
   if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < 0 || variant >= kSorVariants)
     return fail(GPG_ERR_INVALID, "real_size %d ghost %d variant %d", real_size, ghost, variant);
-  g_sor_variant[real_size == 8][ghost] = variant;
+  g_sor_variant[real_size == 8][ghost].store(variant, std::memory_order_relaxed);
   return GPG_OK;
 }
 
@@ -672,7 +675,7 @@ extern "C" int gpg_get_sor_variant(int real_size, int ghost, int *variant) {
   std::call_once(g_tune_once, load_tune_file);
   if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || !variant)
     return fail(GPG_ERR_INVALID, "real_size %d ghost %d", real_size, ghost);
-  *variant = g_sor_variant[real_size == 8][ghost];
+  *variant = g_sor_variant[real_size == 8][ghost].load(std::memory_order_relaxed);
   return GPG_OK;
 }
 
