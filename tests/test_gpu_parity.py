@@ -198,3 +198,30 @@ def test_full_batch_matches_reference_cpu(torch_cuda, rs):
     assert rel_linf(gp, rp) <= TOL[rs]
     same = np.all(gp.reshape(4096, -1) == rp.reshape(4096, -1), axis=1)
     assert same.mean() >= 0.99
+
+
+@pytest.mark.parametrize("scheme,rs,g", [(GPG_SOR, 4, 2), (GPG_SOR, 8, 3), (GPG_MG, 4, 3)])
+def test_non_finite_inputs_follow_oracle(torch_cuda, scheme, rs, g):
+    """A NaN density cell and an infinite coarse-potential cell poison their own
+    patches only, with the oracle's iteration counts: SOR runs them to Max_Iter
+    (the growth test never succeeds on NaN), MG leaves its cycle loop at once
+    (`Error > Tolerated_Error` is false for NaN, CPU_PoissonSolver_MG.cpp:283);
+    every other patch keeps its normal bits."""
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(8, g, seed=1300 + g, dtype=dt)
+    c = d["pot_in"].shape[1] // 2
+    d["rho"][2, 3, 3, 3] = np.nan
+    d["pot_in"][5, c, c, c] = np.inf
+    p = default_params(rs, g, scheme)
+    gp, gf, gi, _ = gpu_run(torch_cuda, p, d)
+    op, of, oi, _ = run_oracle(p, d["rho"], d["pot_in"], flu=d["flu"].copy(), accum_f64=True)
+    assert np.array_equal(gi, oi)
+    if scheme == GPG_SOR:
+        assert gi[2] == p.sor_max_iter and gi[5] == p.sor_max_iter
+    else:
+        assert gi[2] == 1 and gi[5] == 1
+    assert np.isnan(gp[2]).any() and not np.isfinite(gp[5]).all()
+    assert np.array_equal(gp, op, equal_nan=True)
+    assert np.array_equal(gf, of, equal_nan=True)
+    clean = [i for i in range(8) if i not in (2, 5)]
+    assert np.isfinite(gp[clean]).all()
