@@ -12,10 +12,11 @@
 //      in absolute-tolerance mode); cap Max_Iter
 //   c. copy the GRA_NXT^3 window of the cube to pot_out
 //
-// B200 layout.  A team of 1-4 warps owns a patch.  Lane (y, h) owns the
-// interior x-pair {2h+1, 2h+2} of row y at every height and keeps both
-// columns in registers, split by colour: v[c][z] is the lane's colour-c cell
-// at height z (each pair has one cell of each colour per height).  A pass of
+// B200 layout.  A team of 1-8 warps owns a patch.  Lane (y, h) owns the
+// interior x-pair {2h+1, 2h+2} of row y at every height (or, in the
+// column-split variants, at half of the heights) and keeps both columns in
+// registers, split by colour: v[c][z] is the lane's colour-c cell at height z
+// (each pair has one cell of each colour per height).  A pass of
 // colour p updates v[p][z] for all heights and reads
 //   - z neighbours            v[1-p][z+-1]      (own registers)
 //   - one x neighbour         v[1-p][z]         (own registers, the pair mate)
@@ -41,80 +42,119 @@
 namespace gpg {
 
 // Lane mapping and row pitch per (precision, ghost size); see the file comment.
-template <typename T, int G>
+// Z = 1: a lane owns its pair's whole column (heights 1..M).  Z = 2: the column
+// is split in two halves owned by two lanes (heights 1..M/2 and M/2+1..M), so
+// a team has twice the lanes with half the registers each; the lanes of the
+// four (class, half) blocks are packed without padding to half-warps, which
+// fills more of each wavefront where Z = 1 pads (FP64 g3: 576 -> 480
+// wavefronts per patch-sweep, g4: 896 -> 784, FP32 g3: 372 -> 288), at one
+// extra shared load per pass for the neighbour across the split.  R, P, the
+// plane padding PADZ and the block rounding U come from an exhaustive search
+// of a wavefront model (per warp instruction, 32-bit: largest number of
+// distinct words in one bank; 64-bit: the same per half-warp).
+template <typename T, int G, int Z = 1>
 struct SorCfg {
   using g = Geo<G>;
   static constexpr bool F64 = sizeof(T) == 8;
+  static_assert(Z == 1 || Z == 2, "a column is owned by one or two lanes");
+  static constexpr int MH = g::M / Z;  // heights per lane
   // lanes per row (R >= HALF; R > HALF pads rows so wavefronts hold whole rows;
   // FP64 ghost 2 pads its 5-pair rows to 6 lanes, which with P = 11 makes every
   // 64-bit access of a half-warp conflict-free -- with 5 lanes per row the
   // first half-warp of each class took two wavefronts per access)
-  static constexpr int R = (G == 1) ? 4 : (G == 2 ? (F64 ? 6 : 5) : 8);
+  static constexpr int R = (G == 1) ? 4 : (G == 2 ? (F64 ? 6 : 5) : ((G == 3 && Z == 2) ? 6 : 8));
   // row pitch (words), bank-conflict-free choice per configuration
-  static constexpr int P = (G == 1) ? (F64 ? 6 : 12) : (G == 2 ? (F64 ? 11 : 13) : (G == 3 ? (F64 ? 11 : 12) : 12));
+  static constexpr int P = (G == 1) ? ((F64 || Z == 2) ? 6 : 12)
+                                    : (G == 2 ? (F64 ? 11 : 13)
+                                              : (G == 3 ? (F64 ? 11 : (Z == 2 ? 19 : 12)) : 12));
+  static constexpr int PADZ = Z == 1 ? 0 : (G == 3 ? 2 : (G == 4 ? 1 : 0));  // plane padding (words)
+  static constexpr int U = Z == 1 ? 16 : (G == 2 ? (F64 ? 4 : 8) : (G == 3 ? 8 : 1));  // block rounding
   static constexpr int ROWS_PER_CLASS = g::M / 2;
-  static constexpr int CW0 = ((ROWS_PER_CLASS * R + 15) / 16) * 16;
-  static constexpr int TEAM = ((2 * CW0 + 31) / 32) * 32;
-  static constexpr int CW = TEAM / 2;  // lanes per row-parity class
+  static constexpr int BLOCK = ((ROWS_PER_CLASS * R + U - 1) / U) * U;  // lanes per (class, half)
+  static constexpr int TEAM = ((2 * Z * BLOCK + 31) / 32) * 32;
   static constexpr int NWARP = TEAM / 32;
   // every warp holds lanes of one row-parity class only, so the side of a
   // lane's colour-c cell (left / right of its pair) is warp-uniform and the
   // passes are compiled per side.  FP64 only: there it frees registers (FP64
   // g5 phased 202 -> 166, a third team per SM) and each x select is two
   // instructions; the FP32 kernels measured 9-15 % slower at g4/g5 with it.
-  static constexpr bool UNIFORM = F64 && CW % 32 == 0;
-  static constexpr int PP = g::N * P;  // plane pitch
+  static constexpr bool UNIFORM = Z == 1 && F64 && BLOCK % 32 == 0;
+  static constexpr int PP = g::N * P + PADZ;  // plane pitch
   static constexpr int CUBE = 2 * g::N * PP;
   static_assert(R >= g::HALF && P >= g::HALF + 2, "row layout");
+  static_assert(g::M % Z == 0, "column halves");
 
   __device__ static __forceinline__ int addr(int x, int y, int z) {
     return (colour(x, y, z) * g::N + z) * PP + y * P + ((x + 1) >> 1);
   }
 };
 
-template <typename T, int G>
+template <typename T, int G, int Z = 1>
 struct SorSmem {
-  using C = SorCfg<T, G>;
+  using C = SorCfg<T, G, Z>;
   static constexpr size_t round(size_t b) { return (b + 15) / 16 * 16; }
   static constexpr size_t cube_bytes = sizeof(T) * C::CUBE;
   static constexpr size_t part_bytes = sizeof(double) * 2 * C::NWARP;
   static constexpr size_t team_bytes = round(cube_bytes) + round(part_bytes);
 };
 
-// One pass of colour p over every height of the lane's pair: reads the other
-// colour (registers + 3 shared loads per cell), updates v[p][*] in registers,
-// then publishes them.  SUM: accumulate |R| into acc4 (skipped for sweeps
-// whose residual total the stopping rule never looks at).  SIDE: -1 = the
-// lane's side (left_even) is a run-time value; 0 / 1 = it is known at compile
-// time (warp-uniform layouts dispatch once per pass), which turns the x
-// operand selects and the outside-neighbour address into constants.
-template <typename T, int G, bool PHASED, int p, bool SUM, int SIDE>
-__device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2][Geo<G>::M], T *s_cube,
-                                         int own, int xo_even_rt, int xo_odd_rt, bool left_even_rt, T omega_6,
-                                         double (&acc4)[4]) {
-  using C = SorCfg<T, G>;
-  constexpr int N = Geo<G>::N, M = Geo<G>::M, P = C::P, PP = C::PP;
-  const T *nb = s_cube + (1 - p) * N * PP;  // planes of the other colour
-  T *mine = s_cube + p * N * PP;
-  const bool left_even = SIDE < 0 ? left_even_rt : SIDE == 1;
+// A lane's fixed addressing for the passes.  Heights are local to the lane's
+// column half: local zz = 0..MH+1 is global z = zbase + zz, and `zoff` =
+// zbase * PP.  left_even / xo_even / xo_odd refer to the parity of the LOCAL
+// height (for an odd zbase the global parity flips, folded in here).
+struct SorLane {
+  int own;       // in-plane offset of the lane's pair slot
+  int xo_even;   // outside x neighbour slot when (zz + c) is even
+  int xo_odd;    // ... when odd
+  int zoff;      // plane offset of the lane's column half
+  int zh;        // column half (0 / 1); always 0 for Z = 1
+  bool left_even;  // colour-c cell on the left of the pair iff (zz + c) even
+};
+
+// One pass of colour p over every height of the lane's column (half): reads
+// the other colour (registers + 3 shared loads per cell), updates v[p][*] in
+// registers, then publishes them.  SUM: accumulate |R| into acc4 (skipped
+// for sweeps whose residual total the stopping rule never looks at).  SIDE:
+// -1 = the lane's side (left_even) is a run-time value; 0 / 1 = it is known at
+// compile time (warp-uniform layouts dispatch once per pass), which turns the
+// x operand selects and the outside-neighbour address into constants.  With
+// Z = 2 the other-colour neighbour across the split (owned by the other half's
+// lane, updated in the previous pass) is reloaded first.
+template <typename T, int G, int Z, bool PHASED, int p, bool SUM, int SIDE>
+__device__ __forceinline__ void sor_pass(T (&v)[2][SorCfg<T, G, Z>::MH + 2],
+                                         const T (&crho)[2][SorCfg<T, G, Z>::MH], T *s_cube, const SorLane &ln,
+                                         T omega_6, double (&acc4)[4]) {
+  using C = SorCfg<T, G, Z>;
+  constexpr int N = Geo<G>::N, MH = C::MH, P = C::P, PP = C::PP;
+  const int own = ln.own;
+  const T *nb = s_cube + (1 - p) * N * PP + ln.zoff;  // planes of the other colour
+  T *mine = s_cube + p * N * PP + ln.zoff;
+  const bool left_even = SIDE < 0 ? ln.left_even : SIDE == 1;
   // outside x neighbour: slot own-1 for a left cell, own+1 for a right one
-  const int xo_even = SIDE < 0 ? xo_even_rt : (SIDE == 1 ? own - 1 : own + 1);
-  const int xo_odd = SIDE < 0 ? xo_odd_rt : (SIDE == 1 ? own + 1 : own - 1);
+  const int xo_even = SIDE < 0 ? ln.xo_even : (SIDE == 1 ? own - 1 : own + 1);
+  const int xo_odd = SIDE < 0 ? ln.xo_odd : (SIDE == 1 ? own + 1 : own - 1);
+  if constexpr (Z == 2) {
+    const T b = nb[(ln.zh ? 0 : MH + 1) * PP + own];
+    if (ln.zh)
+      v[1 - p][0] = b;
+    else
+      v[1 - p][MH + 1] = b;
+  }
   // all reads of the pass come from the other colour's planes and all writes
-  // go to this colour's planes, so the M updates are independent; the stores
+  // go to this colour's planes, so the MH updates are independent; the stores
   // follow all of them
   if constexpr (PHASED) {
     // phase by phase across all heights, keeping the reference's operand
     // order within each cell
-    T sum[M];
+    T sum[MH];
 #pragma unroll
-    for (int z = 1; z <= M; ++z) sum[z - 1] = add(v[1 - p][z + 1], v[1 - p][z - 1]);
+    for (int z = 1; z <= MH; ++z) sum[z - 1] = add(v[1 - p][z + 1], v[1 - p][z - 1]);
 #pragma unroll
-    for (int z = 1; z <= M; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own + P]);
+    for (int z = 1; z <= MH; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own + P]);
 #pragma unroll
-    for (int z = 1; z <= M; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own - P]);
+    for (int z = 1; z <= MH; ++z) sum[z - 1] = add(sum[z - 1], nb[z * PP + own - P]);
 #pragma unroll
-    for (int z = 1; z <= M; ++z) {
+    for (int z = 1; z <= MH; ++z) {
       const bool even = ((z + p) & 1) == 0;
       const bool left = even == left_even;
       const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
@@ -123,14 +163,14 @@ __device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2
       sum[z - 1] = add(add(sum[z - 1], xp), xm);
     }
 #pragma unroll
-    for (int z = 1; z <= M; ++z) {
+    for (int z = 1; z <= MH; ++z) {
       const T res = sub(sub(sum[z - 1], mul(T(6), v[p][z])), crho[p][z - 1]);
       v[p][z] = add(v[p][z], mul(omega_6, res));
       if constexpr (SUM) acc4[z & 3] += (double)absval(res);
     }
   } else {
 #pragma unroll
-    for (int z = 1; z <= M; ++z) {
+    for (int z = 1; z <= MH; ++z) {
       const bool even = ((z + p) & 1) == 0;
       const bool left = even == left_even;
       const T xo = nb[z * PP + (even ? xo_even : xo_odd)];
@@ -145,20 +185,20 @@ __device__ __forceinline__ void sor_pass(T (&v)[2][Geo<G>::N], const T (&crho)[2
     }
   }
 #pragma unroll
-  for (int z = 1; z <= M; ++z) mine[z * PP + own] = v[p][z];
+  for (int z = 1; z <= MH; ++z) mine[z * PP + own] = v[p][z];
 }
 
-template <typename T, int G, bool PHASED, int p, bool SUM>
-__device__ __forceinline__ void sor_pass_any(T (&v)[2][Geo<G>::N], const T (&crho)[2][Geo<G>::M], T *s_cube,
-                                             int own, int xo_even, int xo_odd, bool left_even, T omega_6,
-                                             double (&acc4)[4]) {
-  if constexpr (SorCfg<T, G>::UNIFORM) {
-    if (left_even)  // warp-uniform branch
-      sor_pass<T, G, PHASED, p, SUM, 1>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+template <typename T, int G, int Z, bool PHASED, int p, bool SUM>
+__device__ __forceinline__ void sor_pass_any(T (&v)[2][SorCfg<T, G, Z>::MH + 2],
+                                             const T (&crho)[2][SorCfg<T, G, Z>::MH], T *s_cube,
+                                             const SorLane &ln, T omega_6, double (&acc4)[4]) {
+  if constexpr (SorCfg<T, G, Z>::UNIFORM) {
+    if (ln.left_even)  // warp-uniform branch
+      sor_pass<T, G, Z, PHASED, p, SUM, 1>(v, crho, s_cube, ln, omega_6, acc4);
     else
-      sor_pass<T, G, PHASED, p, SUM, 0>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      sor_pass<T, G, Z, PHASED, p, SUM, 0>(v, crho, s_cube, ln, omega_6, acc4);
   } else {
-    sor_pass<T, G, PHASED, p, SUM, -1>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    sor_pass<T, G, Z, PHASED, p, SUM, -1>(v, crho, s_cube, ln, omega_6, acc4);
   }
 }
 
@@ -166,39 +206,45 @@ __device__ __forceinline__ void sor_pass_any(T (&v)[2][Geo<G>::N], const T (&crh
 // memory starts at `tb` (SorSmem::team_bytes).  Used by the per-ghost-size
 // kernel below and by the mixed-size persistent kernel (batch_kernel.cuh),
 // so both produce the same bits for a patch.
-template <typename T, int G, bool PHASED>
+template <typename T, int G, bool PHASED, int Z = 1>
 __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P_, int team, int tid,
                                                 unsigned char *tb) {
   using g = Geo<G>;
-  using C = SorCfg<T, G>;
-  using S = SorSmem<T, G>;
+  using C = SorCfg<T, G, Z>;
+  using S = SorSmem<T, G, Z>;
   constexpr int N = g::N, M = g::M, HALF = g::HALF, TEAM = C::TEAM, NWARP = C::NWARP;
-  constexpr int P = C::P, PP = C::PP, R = C::R, CW = C::CW;
-  (void)P;
+  constexpr int P = C::P, PP = C::PP, R = C::R, MH = C::MH, BLOCK = C::BLOCK;
   const int lane = tid & 31, warp = tid >> 5;
   T *s_cube = reinterpret_cast<T *>(tb);
   double *s_part = reinterpret_cast<double *>(tb + S::round(S::cube_bytes));
-
 
   // ---- interpolate the coarse potential into the cube (reads via L1) -----
   interpolate<T, G, TEAM>(a.pot_in + P_ * g::PN3, tid, a.int_scheme,
                           [s_cube](int x, int y, int z, T v) { s_cube[C::addr(x, y, z)] = v; });
   team_sync<TEAM>(team);
 
-  // ---- lane -> (y, h): odd rows in lanes [0, CW), even rows in [CW, 2CW) --
-  const int cls = tid / CW, li = tid - cls * CW, r = li / R, h0 = li - r * R;
-  const bool active = (r < M / 2) && (h0 < HALF);
+  // ---- lane -> (class, half, y, h) ----------------------------------------
+  // blocks of BLOCK lanes: (odd rows, half 0), [(odd rows, half 1)], (even
+  // rows, half 0), [(even rows, half 1)]
+  const int blk = tid / BLOCK, li = tid - blk * BLOCK, r = li / R, h0 = li - r * R;
+  const bool active = (blk < 2 * Z) && (r < M / 2) && (h0 < HALF);
+  const int cls = blk / Z;
   const int y = active ? 2 * r + 1 + cls : 1, h = active ? h0 : 0;
-  const int own = y * P + h + 1;  // in-plane offset of this lane's pair slot
+  const int zbase = active ? (blk - cls * Z) * MH : 0;
   // colour-c cell at height z sits on the left (x = 2h+1) iff (y + z + c) is
   // even; its outside x neighbour is then slot own-1, else own+1.  With y's
   // parity fixed per class the direction is uniform in a wavefront.
-  const bool left_even = !(y & 1);  // left when (z + c) is even
-  const int xo_even = left_even ? own - 1 : own + 1;
-  const int xo_odd = left_even ? own + 1 : own - 1;
+  const bool left_even_g = !(y & 1);  // left when (z + c) is even (global z)
+  SorLane ln;
+  ln.own = y * P + h + 1;
+  ln.left_even = left_even_g != bool(zbase & 1);
+  ln.xo_even = ln.left_even ? ln.own - 1 : ln.own + 1;
+  ln.xo_odd = ln.left_even ? ln.own + 1 : ln.own - 1;
+  ln.zoff = zbase * PP;
+  ln.zh = zbase != 0;
 
-  T v[2][N];
-  T crho[2][M];
+  T v[2][MH + 2];
+  T crho[2][MH];
   double cr_sum = 0.0;
   {
     const T *rho = a.rho + P_ * g::RHO3;
@@ -206,15 +252,16 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
 #pragma unroll
-      for (int z = 0; z < N; ++z) v[c][z] = s_cube[(c * N + z) * PP + own];
+      for (int zz = 0; zz < MH + 2; ++zz) v[c][zz] = s_cube[(c * N + zbase + zz) * PP + ln.own];
 #pragma unroll
-      for (int z = 1; z <= M; ++z) {
-        const bool left = (((z + c) & 1) == 0) == left_even;
+      for (int zz = 1; zz <= MH; ++zz) {
+        const int z = zbase + zz;
+        const bool left = (((z + c) & 1) == 0) == left_even_g;
         const int x = left ? 2 * h + 1 : 2 * h + 2;
         const int idx = ((z - 1) * M + (y - 1)) * M + (x - 1);
-        crho[c][z - 1] = active ? mul(a.sor_const, __ldg(rho + idx)) : T(0);
-        cr_sum += (double)absval(crho[c][z - 1]);
-        if (a.init_mode != 0) v[c][z] = (a.init_mode == 2 && active) ? __ldg(guess + idx) : T(0);
+        crho[c][zz - 1] = active ? mul(a.sor_const, __ldg(rho + idx)) : T(0);
+        cr_sum += (double)absval(crho[c][zz - 1]);
+        if (a.init_mode != 0) v[c][zz] = (a.init_mode == 2 && active) ? __ldg(guess + idx) : T(0);
       }
     }
   }
@@ -223,7 +270,7 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
-      for (int z = 1; z <= M; ++z) s_cube[(c * N + z) * PP + own] = v[c][z];
+      for (int zz = 1; zz <= MH; ++zz) s_cube[(c * N + zbase + zz) * PP + ln.own] = v[c][zz];
   }
   double tol_abs = 0.0;
   if (a.stop_mode == 1) {
@@ -257,15 +304,15 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
     // deterministic and identical for a patch solved alone or in a batch
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
     if (!need) {
-      if (active) sor_pass_any<T, G, PHASED, 0, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      if (active) sor_pass_any<T, G, Z, PHASED, 0, false>(v, crho, s_cube, ln, omega_6, acc4);
       team_sync<TEAM>(team);
-      if (active) sor_pass_any<T, G, PHASED, 1, false>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+      if (active) sor_pass_any<T, G, Z, PHASED, 1, false>(v, crho, s_cube, ln, omega_6, acc4);
       team_sync<TEAM>(team);
       continue;
     }
-    if (active) sor_pass_any<T, G, PHASED, 0, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    if (active) sor_pass_any<T, G, Z, PHASED, 0, true>(v, crho, s_cube, ln, omega_6, acc4);
     team_sync<TEAM>(team);
-    if (active) sor_pass_any<T, G, PHASED, 1, true>(v, crho, s_cube, own, xo_even, xo_odd, left_even, omega_6, acc4);
+    if (active) sor_pass_any<T, G, Z, PHASED, 1, true>(v, crho, s_cube, ln, omega_6, acc4);
     double acc = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
     acc = warp_sum(acc);
     if constexpr (NWARP > 1) {
@@ -309,19 +356,20 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
   }
 }
 
-// PPC: teams (patches) per CTA.  PHASED: form the M independent updates of a
+// PPC: teams (patches) per CTA.  PHASED: form the MH independent updates of a
 // pass phase by phase across heights (more updates in flight, more registers)
-// instead of height by height.  Both orders give identical bits; the
-// autotuner (gpg_set_sor_variant) picks per (precision, ghost size).
-template <typename T, int G, int PPC, bool PHASED>
-__global__ void __launch_bounds__(PPC *SorCfg<T, G>::TEAM)
+// instead of height by height.  Z: lanes per pair column (1 or 2).  Every
+// variant gives identical bits; the autotuner (gpg_set_sor_variant) picks per
+// (precision, ghost size).
+template <typename T, int G, int PPC, bool PHASED, int Z = 1>
+__global__ void __launch_bounds__(PPC *SorCfg<T, G, Z>::TEAM)
     sor_kernel(const SolveArgs<T> a) {
-  constexpr int TEAM = SorCfg<T, G>::TEAM;
+  constexpr int TEAM = SorCfg<T, G, Z>::TEAM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int team = threadIdx.x / TEAM, tid = threadIdx.x - team * TEAM;
   const int64_t P_ = int64_t(blockIdx.x) * PPC + team;
   if (P_ >= a.npatch) return;  // whole team leaves together
-  sor_solve_patch<T, G, PHASED>(a, P_, team, tid, smem_raw + team * SorSmem<T, G>::team_bytes);
+  sor_solve_patch<T, G, PHASED, Z>(a, P_, team, tid, smem_raw + team * SorSmem<T, G, Z>::team_bytes);
 }
 
 }  // namespace gpg

@@ -1,5 +1,7 @@
-"""Every SOR kernel variant (patches per CTA x pass order) returns the same
-bits as every other (needs a B200)."""
+"""Every SOR kernel variant (patches per CTA x pass order x lanes per pair
+column) returns the same bits as every other (needs a B200).  The column-split
+variants sum the residual in another order; on these inputs every total and
+sweep count still agrees bit for bit."""
 import ctypes as C
 
 import numpy as np
