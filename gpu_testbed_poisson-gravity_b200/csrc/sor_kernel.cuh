@@ -358,9 +358,10 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
 
 // PPC: teams (patches) per CTA.  PHASED: form the MH independent updates of a
 // pass phase by phase across heights (more updates in flight, more registers)
-// instead of height by height.  Z: lanes per pair column (1 or 2).  Every
-// variant gives identical bits; the autotuner (gpg_set_sor_variant) picks per
-// (precision, ghost size).
+// instead of height by height.  Z: lanes per pair column (1 or 2).  The Z = 1
+// variants give identical bits; Z = 2 sums the residual in another order (the
+// fields are the same whenever the sweep counts are).  The autotuner
+// (gpg_set_sor_variant) picks per (precision, ghost size).
 template <typename T, int G, int PPC, bool PHASED, int Z = 1>
 __global__ void __launch_bounds__(PPC *SorCfg<T, G, Z>::TEAM)
     sor_kernel(const SolveArgs<T> a) {
