@@ -621,6 +621,9 @@ def main(argv=None) -> int:
         keep = {}
         v, cores, kind, sample = reference_cpu(batches, budget_s=20.0, keep=keep)
         line["cpu_baseline"] = {"value": v, "unit": "patches/s", "cores": cores, "kind": kind, "sample": sample}
+        # the same code on one core (smaller sample): the per-core cost of the reference
+        v1, _, _, sample1 = reference_cpu(batches, budget_s=6.0, nthreads=1)
+        line["cpu_baseline"]["one_core"] = {"value": v1, "unit": "patches/s", "cores": 1, "sample": sample1}
         line["errors"] = headline_errors(torch, batches, dev_in, keep)
     if rank == 0 and not a.no_extra and not a.only and world == 1:
         line["extra"] = extra_configs(torch, dev, cpu=not a.no_cpu_baseline)
