@@ -10,7 +10,10 @@ patch box and the matching analytic coarse potential (gpg.inputs).
 
 Reported (one JSON line from rank 0):
   value      patches/s over the whole job, inputs resident in HBM (device timing,
-             CUDA events on the launching stream, max over ranks)
+             CUDA events on the timing stream, max over ranks); the 8 batches
+             run on their own streams, forked from and joined to the timing
+             stream; value_one_stream times the same steps one launch at a time,
+             and that pass gives the per-kernel times (per_batch_ms, roofline)
   e2e        the same through the reference-shaped host API (pinned host
              buffers, H2D + solve + D2H per step; host clock around a full sync;
              batches pipelined across steps, lockstep_value with a full sync
@@ -397,6 +400,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="gpg", choices=["gpg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--one-stream", action="store_true",
+                    help="time the step with its batches one after another on one stream")
     ap.add_argument("--no-extra", action="store_true", help="skip the other configurations (MG, mixed batch, learned guess)")
     ap.add_argument("--only", default=None,
                     help="comma list of batches to run (e.g. f64_g5); profiling cases, not a bench line")
@@ -455,8 +460,23 @@ def main(argv=None) -> int:
                            resid=torch.empty(n, dtype=torch.float64, device=dev)))
     stream = torch.cuda.current_stream(dev)
     step_inputs = sum((d["rho"].nbytes + d["pot_in"].nbytes) for _, d in batches)
+    # one stream per batch: the batches are independent, so a batch's first
+    # patches run while the previous one's last patches finish
+    side = [torch.cuda.Stream(dev) for _ in batches]
 
-    def step(events=None):
+    def step_concurrent():
+        fork = torch.cuda.Event()
+        fork.record(stream)
+        for (p, _), t, st in zip(batches, dev_in, side):
+            st.wait_event(fork)
+            solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], iters=t["iters"], resid=t["resid"],
+                         stream=st)
+        for st in side:
+            join = torch.cuda.Event()
+            join.record(st)
+            stream.wait_event(join)
+
+    def step_sequential(events=None):
         for k, ((p, _), t) in enumerate(zip(batches, dev_in)):
             if events is not None:
                 events[k][0].record(stream)
@@ -464,6 +484,7 @@ def main(argv=None) -> int:
             if events is not None:
                 events[k][1].record(stream)
 
+    step = step_sequential if a.one_stream else step_concurrent
     for _ in range(max(a.warmup, 3)):
         step()
     torch.cuda.synchronize(dev)
@@ -476,21 +497,31 @@ def main(argv=None) -> int:
     ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in batches]
           for _ in range(a.steps)]
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_start, s_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clk:
         barrier()
         start.record(stream)
         for s in range(a.steps):
-            step(ev[s])
+            step()
         stop.record(stream)
         barrier()
+        # the same steps one launch at a time on one stream: per-kernel times
+        # (roofline, per-batch fractions) without overlap between kernels
+        s_start.record(stream)
+        for s in range(a.steps):
+            step_sequential(ev[s])
+        s_stop.record(stream)
+        barrier()
     ms = start.elapsed_time(stop)
+    ms_seq = s_start.elapsed_time(s_stop)
     per_kernel = np.array([[e[0].elapsed_time(e[1]) for e in row] for row in ev])  # [steps, batches]
     if world > 1:
-        t = torch.tensor([ms], device=dev)
+        t = torch.tensor([ms, ms_seq], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms, ms_seq = float(t[0].item()), float(t[1].item())
     patches_step = NPATCH * len(batches)
     value = world * patches_step * a.steps / (ms / 1e3)
+    value_one_stream = world * patches_step * a.steps / (ms_seq / 1e3)
     iters = [t["iters"].cpu().numpy() for t in dev_in]
 
     # ---- end to end through the reference-shaped host API ----------------
@@ -601,6 +632,8 @@ def main(argv=None) -> int:
                    "parallelism": f"patch shards x{world}",
                    "learned_init": "extra.learned_init_sor_g1 (ghost 1, 65536 held-out patches)"},
         "gpu_launches": len(batches) * a.steps,
+        "batches": "one stream" if a.one_stream else "one stream per batch, forked from and joined to the timing stream",
+        "value_one_stream": value_one_stream,
         "per_batch_ms": {f"f{8 * p.real_size}_g{p.ghost}": float(per_kernel[:, i].mean())
                          for i, (p, _) in enumerate(batches)},
         "mean_iters": {f"f{8 * p.real_size}_g{p.ghost}": float(it.mean()) for (p, _), it in zip(batches, iters)},
@@ -613,6 +646,7 @@ def main(argv=None) -> int:
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
                      "launch_ms": launch_ms, "peak_source": "measured" if peaks else "fallback",
+                     "launch_timing": "CUDA events around each launch in the one-stream pass of the same steps",
                      "onchip": onchip},
         "e2e": e2e,
         "clocks": clocks,
