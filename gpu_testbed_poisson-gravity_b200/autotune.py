@@ -27,14 +27,14 @@ from gpg.lib import GpgError, check, library, solve_device  # noqa: E402
 
 
 def variants():
-    """(variant, patches per CTA, phased pass, lanes per pair column) for every variant."""
+    """(variant, patches per CTA, phased pass, lanes per pair column, rows per lane)."""
     lib = library()
     out = []
     for v in range(lib.gpg_sor_variant_count()):
-        ppc, ph, z = C.c_int(), C.c_int(), C.c_int()
+        ppc, ph, z, y = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         check(lib.gpg_sor_variant_info(v, C.byref(ppc), C.byref(ph)))
-        check(lib.gpg_sor_variant_split(v, C.byref(z)))
-        out.append((v, ppc.value, bool(ph.value), z.value))
+        check(lib.gpg_sor_variant_layout(v, C.byref(z), C.byref(y)))
+        out.append((v, ppc.value, bool(ph.value), z.value, y.value))
     return out
 
 
@@ -70,7 +70,7 @@ def tune(npatch=4096, precisions=(4, 8), ghosts=(1, 2, 3, 4, 5)):
             cur = C.c_int()
             check(lib.gpg_get_sor_variant(rs, g, C.byref(cur)))
             times, ref = {}, None
-            for v, ppc, ph, z in variants():
+            for v, ppc, ph, z, y in variants():
                 check(lib.gpg_set_sor_variant(rs, g, v))
                 try:
                     ms = time_variant(torch, p, t)

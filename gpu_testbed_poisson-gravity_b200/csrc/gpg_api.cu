@@ -79,15 +79,17 @@ int ensure_smem(KernelFn *fn, size_t bytes, AttrOnce &st) {
 // SOR kernel variants: (teams per CTA, phased pass).  The table below holds
 // the variant per (precision, ghost size); defaults are the fastest measured
 // on B200, gpg_set_sor_variant / a tuning file override them.
-constexpr int kSorVariants = 10;
-constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4, 1, 1, 2, 2};
-constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true, false, true, false, true};
-constexpr int kSorVariantSplit[kSorVariants] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 2};  // lanes per pair column
+constexpr int kSorVariants = 14;
+constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4, 1, 1, 2, 2, 1, 1, 1, 1};
+constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true, false,
+                                                  true,  false, true, false, true, false, true};
+constexpr int kSorVariantSplit[kSorVariants] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 1, 1};  // lanes per column
+constexpr int kSorVariantRows[kSorVariants] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2};   // rows per lane
 // atomic: gpg_set_sor_variant may run on one host thread while another launches
 std::atomic<int> g_sor_variant[2][6] = {
     // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
-    {0, 1, 0, 6, 6, 7},   // float
-    {0, 1, 0, 7, 1, 0},   // double
+    {0, 10, 11, 10, 11, 10},   // float
+    {0, 11, 13, 11, 10, 11},   // double
 };
 std::once_flag g_tune_once;
 
@@ -118,53 +120,65 @@ void load_tune_file() {
   std::fclose(f);
 }
 
-template <typename T, int G, int PPC, bool PHASED, int Z>
+template <typename T, int G, int PPC, bool PHASED, int Z, int Y>
 AttrOnce &sor_attr() {
   static AttrOnce attr;
   return attr;
 }
 
-template <typename T, int G, int PPC, bool PHASED, int Z>
+template <typename T, int G, int PPC, bool PHASED, int Z, int Y>
 int launch_sor_v(const gpg::SolveArgs<T> &a, cudaStream_t s) {
-  using S = gpg::SorSmem<T, G, Z>;
-  constexpr int threads = PPC * gpg::SorCfg<T, G, Z>::TEAM;
-  const size_t smem = PPC * S::team_bytes;
-  if (smem > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %zu bytes of shared memory", smem);
-  auto fn = gpg::sor_kernel<T, G, PPC, PHASED, Z>;
-  AttrOnce &attr = sor_attr<T, G, PPC, PHASED, Z>();
-  if (int rc = ensure_smem(fn, smem, attr)) return rc;
-  if (threads > attr.max_threads)
-    return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %d threads per CTA (registers allow %d)", threads,
-                attr.max_threads);
-  const int64_t grid = (a.npatch + PPC - 1) / PPC;
-  fn<<<(unsigned)grid, threads, smem, s>>>(a);
-  GPG_CUDA(cudaGetLastError());
-  return GPG_OK;
+  if constexpr (!gpg::SorCfg<T, G, Z, Y>::FITS) {
+    return fail(GPG_ERR_UNSUPPORTED, "SOR variant holds more state per lane than registers allow");
+  } else {
+    using S = gpg::SorSmem<T, G, Z, Y>;
+    constexpr int threads = PPC * gpg::SorCfg<T, G, Z, Y>::TEAM;
+    const size_t smem = PPC * S::team_bytes;
+    if (smem > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %zu bytes of shared memory", smem);
+    auto fn = gpg::sor_kernel<T, G, PPC, PHASED, Z, Y>;
+    AttrOnce &attr = sor_attr<T, G, PPC, PHASED, Z, Y>();
+    if (int rc = ensure_smem(fn, smem, attr)) return rc;
+    if (threads > attr.max_threads)
+      return fail(GPG_ERR_UNSUPPORTED, "SOR variant needs %d threads per CTA (registers allow %d)", threads,
+                  attr.max_threads);
+    const int64_t grid = (a.npatch + PPC - 1) / PPC;
+    fn<<<(unsigned)grid, threads, smem, s>>>(a);
+    GPG_CUDA(cudaGetLastError());
+    return GPG_OK;
+  }
 }
 
 // Kernel attributes of the SOR variant a (precision, ghost) solve will launch,
 // set without launching (stream capture must not see first-use set-up).
-template <typename T, int G, int PPC, bool PHASED, int Z>
+template <typename T, int G, int PPC, bool PHASED, int Z, int Y>
 int prepare_sor_v() {
-  auto fn = gpg::sor_kernel<T, G, PPC, PHASED, Z>;
-  static AttrOnce &attr = sor_attr<T, G, PPC, PHASED, Z>();
-  return ensure_smem(fn, PPC * gpg::SorSmem<T, G, Z>::team_bytes, attr);
+  if constexpr (!gpg::SorCfg<T, G, Z, Y>::FITS) {
+    return fail(GPG_ERR_UNSUPPORTED, "SOR variant holds more state per lane than registers allow");
+  } else {
+    auto fn = gpg::sor_kernel<T, G, PPC, PHASED, Z, Y>;
+    static AttrOnce &attr = sor_attr<T, G, PPC, PHASED, Z, Y>();
+    return ensure_smem(fn, PPC * gpg::SorSmem<T, G, Z, Y>::team_bytes, attr);
+  }
 }
 
 template <typename T, int G>
 int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   std::call_once(g_tune_once, load_tune_file);
   switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
-    case 0: return launch_sor_v<T, G, 1, false, 1>(a, s);
-    case 1: return launch_sor_v<T, G, 1, true, 1>(a, s);
-    case 2: return launch_sor_v<T, G, 2, false, 1>(a, s);
-    case 3: return launch_sor_v<T, G, 2, true, 1>(a, s);
-    case 4: return launch_sor_v<T, G, 4, false, 1>(a, s);
-    case 5: return launch_sor_v<T, G, 4, true, 1>(a, s);
-    case 6: return launch_sor_v<T, G, 1, false, 2>(a, s);
-    case 7: return launch_sor_v<T, G, 1, true, 2>(a, s);
-    case 8: return launch_sor_v<T, G, 2, false, 2>(a, s);
-    default: return launch_sor_v<T, G, 2, true, 2>(a, s);
+    case 0: return launch_sor_v<T, G, 1, false, 1, 1>(a, s);
+    case 1: return launch_sor_v<T, G, 1, true, 1, 1>(a, s);
+    case 2: return launch_sor_v<T, G, 2, false, 1, 1>(a, s);
+    case 3: return launch_sor_v<T, G, 2, true, 1, 1>(a, s);
+    case 4: return launch_sor_v<T, G, 4, false, 1, 1>(a, s);
+    case 5: return launch_sor_v<T, G, 4, true, 1, 1>(a, s);
+    case 6: return launch_sor_v<T, G, 1, false, 2, 1>(a, s);
+    case 7: return launch_sor_v<T, G, 1, true, 2, 1>(a, s);
+    case 8: return launch_sor_v<T, G, 2, false, 2, 1>(a, s);
+    case 9: return launch_sor_v<T, G, 2, true, 2, 1>(a, s);
+    case 10: return launch_sor_v<T, G, 1, false, 2, 2>(a, s);
+    case 11: return launch_sor_v<T, G, 1, true, 2, 2>(a, s);
+    case 12: return launch_sor_v<T, G, 1, false, 1, 2>(a, s);
+    default: return launch_sor_v<T, G, 1, true, 1, 2>(a, s);
   }
 }
 
@@ -172,16 +186,20 @@ template <typename T, int G>
 int prepare_sor() {
   std::call_once(g_tune_once, load_tune_file);
   switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
-    case 0: return prepare_sor_v<T, G, 1, false, 1>();
-    case 1: return prepare_sor_v<T, G, 1, true, 1>();
-    case 2: return prepare_sor_v<T, G, 2, false, 1>();
-    case 3: return prepare_sor_v<T, G, 2, true, 1>();
-    case 4: return prepare_sor_v<T, G, 4, false, 1>();
-    case 5: return prepare_sor_v<T, G, 4, true, 1>();
-    case 6: return prepare_sor_v<T, G, 1, false, 2>();
-    case 7: return prepare_sor_v<T, G, 1, true, 2>();
-    case 8: return prepare_sor_v<T, G, 2, false, 2>();
-    default: return prepare_sor_v<T, G, 2, true, 2>();
+    case 0: return prepare_sor_v<T, G, 1, false, 1, 1>();
+    case 1: return prepare_sor_v<T, G, 1, true, 1, 1>();
+    case 2: return prepare_sor_v<T, G, 2, false, 1, 1>();
+    case 3: return prepare_sor_v<T, G, 2, true, 1, 1>();
+    case 4: return prepare_sor_v<T, G, 4, false, 1, 1>();
+    case 5: return prepare_sor_v<T, G, 4, true, 1, 1>();
+    case 6: return prepare_sor_v<T, G, 1, false, 2, 1>();
+    case 7: return prepare_sor_v<T, G, 1, true, 2, 1>();
+    case 8: return prepare_sor_v<T, G, 2, false, 2, 1>();
+    case 9: return prepare_sor_v<T, G, 2, true, 2, 1>();
+    case 10: return prepare_sor_v<T, G, 1, false, 2, 2>();
+    case 11: return prepare_sor_v<T, G, 1, true, 2, 2>();
+    case 12: return prepare_sor_v<T, G, 1, false, 1, 2>();
+    default: return prepare_sor_v<T, G, 1, true, 1, 2>();
   }
 }
 
@@ -673,9 +691,10 @@ extern "C" int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phas
   return GPG_OK;
 }
 
-extern "C" int gpg_sor_variant_split(int variant, int *lanes_per_column) {
+extern "C" int gpg_sor_variant_layout(int variant, int *lanes_per_column, int *rows_per_lane) {
   if (variant < 0 || variant >= kSorVariants) return fail(GPG_ERR_INVALID, "variant %d", variant);
   if (lanes_per_column) *lanes_per_column = kSorVariantSplit[variant];
+  if (rows_per_lane) *rows_per_lane = kSorVariantRows[variant];
   return GPG_OK;
 }
 

@@ -229,16 +229,19 @@ GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
 /* ---------------------------------------------------------------------------
  * SOR kernel variants.  No reference counterpart (the reference fixes its
  * launch shape per ghost size with macros, Header/CUPOT.h:44-90).  A variant
- * is (patches per CTA, phased pass order, lanes per pair column): variants
- * 0-5 give each lane a whole column of heights, 6-9 split it between two
- * lanes (twice the threads, half the registers each).  Results are
- * bit-identical across variants.  The table starts from the library's defaults, then an optional
+ * is (patches per CTA, phased pass order, lanes per pair column, rows per
+ * lane): variants 0-5 give each lane a whole column of one row, 6-9 split the
+ * column between two lanes (twice the threads, half the registers each),
+ * 10-11 give a lane two rows and half a column, 12-13 two rows and a whole
+ * column (not built where that exceeds the register file: GPG_ERR_UNSUPPORTED).
+ * Variants 0-5 return identical bits; the others sum the residual in another
+ * order, so a stop decision can differ only where two sweeps' totals tie.  The table starts from the library's defaults, then an optional
  * tuning file ($GPG_TUNE_FILE, else sor_tune.txt beside libgpg.so, lines
  * "f32|f64 <ghost> <variant>") written by autotune.py.
  * ------------------------------------------------------------------------- */
 GPG_API int gpg_sor_variant_count(void);
 GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased);
-GPG_API int gpg_sor_variant_split(int variant, int *lanes_per_column);
+GPG_API int gpg_sor_variant_layout(int variant, int *lanes_per_column, int *rows_per_lane);
 GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
 GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
 
