@@ -20,8 +20,9 @@ Reported (one JSON line from rank 0):
              after every step)
   roofline   dominant kernel: compulsory HBM bytes per launch / mean launch time;
              roofline.onchip: its shared-memory wavefronts per launch (measured
-             sweeps x 3 loads + 1 store per cell update) / launch time, against
-             one wavefront per cycle per SM at the sampled clock
+             sweeps x cell updates x the shared accesses per update of the
+             kernel's layout) / launch time, against one wavefront per cycle
+             per SM at the sampled clock
   cpu_baseline  the reference's own CPU code (oracle/_ref, all host threads) on
              a bounded sample of the same workload
 `--impl reference` runs only the reference CPU path (rank 0) and prints its line.
@@ -602,23 +603,42 @@ def main(argv=None) -> int:
     except OSError:
         pass
 
-    # on-chip bound of the same kernel: every cell update is 3 shared loads + 1
-    # shared store; a warp-wide access of 4-byte (8-byte) values is 1 (2)
-    # shared-memory wavefronts; the pipe serves one wavefront per cycle per SM
+    # on-chip bound of the same kernel: the shared-memory accesses one cell
+    # update needs in the layout the kernel runs (one row per lane: 3 loads +
+    # 1 store; two rows per lane: 2 loads + 1 store; a column split between
+    # two lanes adds one load per lane, row and pass); a warp-wide access of
+    # 4-byte (8-byte) values is 1 (2) wavefronts; the pipe serves one wavefront
+    # per cycle per SM
     clocks = clk.summary()
     sm_mhz = float(clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0))
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
-    g = pk.ghost
-    cell_updates = float(iters[k].astype(np.float64).sum()) * (6 + 2 * g) ** 3
-    wavefronts = cell_updates * 4 * (pk.real_size * 32 // 128) / 32
     onchip_peak = nsm * sm_mhz * 1e6
+
+    def layout(p):
+        import ctypes as C
+        from gpg.lib import check
+        lib = library()
+        v, z, y = C.c_int(), C.c_int(), C.c_int()
+        check(lib.gpg_get_sor_variant(p.real_size, p.ghost, C.byref(v)))
+        check(lib.gpg_sor_variant_layout(v.value, C.byref(z), C.byref(y)))
+        m = 6 + 2 * p.ghost
+        acc = (4.0 if y.value == 1 else 3.0) + (1.0 / (m // z.value) if z.value == 2 else 0.0)
+        return v.value, z.value, y.value, acc
+
+    def wavefronts_of(p, it):
+        acc = layout(p)[3]
+        return float(it.astype(np.float64).sum()) * (6 + 2 * p.ghost) ** 3 * acc * (p.real_size * 32 // 128) / 32
+
+    wavefronts = wavefronts_of(pk, iters[k])
+    vk, zk, yk, acck = layout(pk)
     onchip = {"resource": "shared-memory pipe", "unit": "wavefronts/s",
               "achieved": wavefronts / (launch_ms / 1e3), "peak": onchip_peak,
               "frac": wavefronts / (launch_ms / 1e3) / onchip_peak,
               "algorithmic_wavefronts_per_launch": wavefronts,
               "achieved_gbs": wavefronts * 128 / (launch_ms / 1e3) / 1e9, "peak_gbs": onchip_peak * 128 / 1e9,
-              "model": "measured sweeps x RHO_NXT^3 cell updates x (3 loads + 1 store); 1 wavefront "
-                       "(128 B)/cycle/SM "
+              "variant": {"id": vk, "lanes_per_column": zk, "rows_per_lane": yk},
+              "model": f"measured sweeps x RHO_NXT^3 cell updates x {acck:.3f} shared accesses per update "
+                       "(this variant's layout); 1 wavefront (128 B)/cycle/SM "
                        f"at the sampled {sm_mhz:.0f} MHz x {nsm} SMs"}
 
     line = {
@@ -638,9 +658,7 @@ def main(argv=None) -> int:
                          for i, (p, _) in enumerate(batches)},
         "mean_iters": {f"f{8 * p.real_size}_g{p.ghost}": float(it.mean()) for (p, _), it in zip(batches, iters)},
         "onchip_frac_per_batch": {
-            f"f{8 * p.real_size}_g{p.ghost}":
-                float(it.astype(np.float64).sum()) * (6 + 2 * p.ghost) ** 3 * 4 * (p.real_size * 32 // 128) / 32
-                / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
+            f"f{8 * p.real_size}_g{p.ghost}": wavefronts_of(p, it) / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
             for i, ((p, _), it) in enumerate(zip(batches, iters))},
         "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
