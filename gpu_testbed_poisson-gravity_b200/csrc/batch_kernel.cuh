@@ -6,9 +6,12 @@
 // by group with the largest cubes first.  Every CTA of 128 threads takes the
 // next unit from a device counter (one atomicAdd per unit), solves it and
 // asks again, so patches whose sweep counts differ by 10x still keep all SMs
-// busy to the end.  Each patch runs sor_solve_patch with the same team shape
-// and lane mapping as the per-ghost-size kernel, hence the same bits as when
-// it is solved alone.
+// busy to the end.  Each patch runs sor_solve_patch with the team shape and
+// lane mapping of one of the per-ghost-size variants: two rows per lane and
+// half a column in FP32 (teams of 32-128 threads, as in the fastest FP32
+// variants), one row and a whole column in FP64 (the two-row FP64 layouts hold
+// more registers than three resident CTAs allow).  The fields equal those of
+// a patch solved alone whenever the sweep counts do.
 #pragma once
 
 #include "sor_kernel.cuh"
@@ -18,11 +21,20 @@ namespace gpg {
 constexpr int kBatchMaxGroups = 8;
 constexpr int kBatchThreads = 128;
 
+// lane layout of the batch kernel: (lanes per pair column, rows per lane)
+template <typename T>
+struct BatchLayout {
+  static constexpr int Z = sizeof(T) == 4 ? 2 : 1;
+  static constexpr int Y = sizeof(T) == 4 ? 2 : 1;
+};
+
 template <typename T, int G>
 struct BatchUnit {
-  static constexpr int TEAM = SorCfg<T, G>::TEAM;
+  using L = BatchLayout<T>;
+  static constexpr int TEAM = SorCfg<T, G, L::Z, L::Y>::TEAM;
   static constexpr int TEAMS = kBatchThreads / TEAM;  // patches per unit
-  static constexpr size_t smem = TEAMS * SorSmem<T, G>::team_bytes;
+  static constexpr size_t team_bytes = SorSmem<T, G, L::Z, L::Y>::team_bytes;
+  static constexpr size_t smem = TEAMS * team_bytes;
   static_assert(TEAMS >= 1, "team larger than a batch CTA");
 };
 
@@ -44,7 +56,8 @@ __device__ __forceinline__ void batch_unit(const SolveArgs<T> &a, int64_t unit_i
   const int tid = threadIdx.x - team * U::TEAM;
   const int64_t P = unit_in_group * U::TEAMS + team;
   if (P >= a.npatch) return;     // last unit of a group may be partial
-  sor_solve_patch<T, G, false>(a, P, team, tid, smem + team * SorSmem<T, G>::team_bytes);
+  using L = BatchLayout<T>;
+  sor_solve_patch<T, G, false, L::Z, L::Y>(a, P, team, tid, smem + team * U::team_bytes);
 }
 
 // Resident CTAs per SM the register allocation must allow (the five ghost
