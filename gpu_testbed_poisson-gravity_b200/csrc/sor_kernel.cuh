@@ -83,7 +83,7 @@ struct SorCfg {
   static constexpr int U = Y == 1 ? (Z == 1 ? 16 : (G == 2 ? (F64 ? 4 : 8) : (G == 3 ? 8 : 1)))
                                   : (Z == 1 ? 1
                                             : (G == 2 ? (F64 ? 4 : 8)
-                                                      : (G == 3 ? (F64 ? 8 : 1) : ((G == 4 && !F64) ? 16 : 1))));
+                                                      : (G == 3 ? (F64 ? 8 : 1) : (G == 4 ? (F64 ? 32 : 16) : 1))));
   static constexpr int ROWS = g::M / 2;  // rows per parity class (Y = 1) = row pairs (Y = 2)
   // lanes per block: (class, half) blocks for Y = 1, (half) blocks for Y = 2
   static constexpr int BLOCK = ((ROWS * R + U - 1) / U) * U;
@@ -96,6 +96,9 @@ struct SorCfg {
   // (FP64 g5 phased 202 -> 166, a third team per SM) and each x select is two
   // instructions; the FP32 kernels measured 9-15 % slower at g4/g5 with it.
   static constexpr bool UNIFORM = Y == 1 && Z == 1 && F64 && BLOCK % 32 == 0;
+  // Y = 2 with an odd MH: the upper half's cells sit on the other side; with
+  // whole warps per half that side is warp-uniform and compiled per half
+  static constexpr bool HALF_UNIFORM = Y == 2 && Z == 2 && (MH & 1) && BLOCK % 32 == 0;
   static constexpr int PP = g::N * P + PADZ;  // plane pitch
   static constexpr int CUBE = 2 * g::N * PP;
   // register words of a lane's columns and Const*rho; layouts far beyond the
@@ -225,7 +228,7 @@ __device__ __forceinline__ void sor_pass(T (&vv)[1][2][SorCfg<T, G, Z>::MH + 2],
 // (x0, y1) = v[1][1-p]: the x mate of one cell and the in-lane y neighbour of
 // the other.  Shared memory supplies the y0-1 / y1+1 neighbours and the two
 // outside x neighbours.  Operand order per cell as the reference's.
-template <typename T, int G, int Z, bool PHASED, int p, bool SUM>
+template <typename T, int G, int Z, bool PHASED, int p, bool SUM, int SIDE>
 __device__ __forceinline__ void sor_pass2(T (&v)[2][2][SorCfg<T, G, Z, 2>::MH + 2],
                                           const T (&crho)[2][2][SorCfg<T, G, Z, 2>::MH], T *s_cube,
                                           const SorLane &ln, T omega_6, double (&acc4)[4]) {
@@ -239,7 +242,7 @@ __device__ __forceinline__ void sor_pass2(T (&v)[2][2][SorCfg<T, G, Z, 2>::MH + 
   // row y0's is then on the right; left_even is true at compile time unless an
   // odd MH makes it depend on the column half
   constexpr bool RT = (Z == 2) && (MH & 1);
-  const bool le = RT ? ln.left_even : true;
+  const bool le = SIDE >= 0 ? SIDE == 1 : (RT ? ln.left_even : true);
   // sum of the six neighbours of row r's colour-p cell at height z; yreg is
   // the y neighbour held in registers (y0+1 for row 0, y1-1 for row 1), ysm
   // the one read from shared memory
@@ -302,7 +305,14 @@ __device__ __forceinline__ void sor_pass_any(T (&v)[Y][2][SorCfg<T, G, Z, Y>::MH
                                              const T (&crho)[Y][2][SorCfg<T, G, Z, Y>::MH], T *s_cube,
                                              const SorLane &ln, T omega_6, double (&acc4)[4]) {
   if constexpr (Y == 2) {
-    sor_pass2<T, G, Z, PHASED, p, SUM>(v, crho, s_cube, ln, omega_6, acc4);
+    if constexpr (SorCfg<T, G, Z, Y>::HALF_UNIFORM) {
+      if (ln.left_even)  // warp-uniform branch
+        sor_pass2<T, G, Z, PHASED, p, SUM, 1>(v, crho, s_cube, ln, omega_6, acc4);
+      else
+        sor_pass2<T, G, Z, PHASED, p, SUM, 0>(v, crho, s_cube, ln, omega_6, acc4);
+    } else {
+      sor_pass2<T, G, Z, PHASED, p, SUM, -1>(v, crho, s_cube, ln, omega_6, acc4);
+    }
   } else if constexpr (SorCfg<T, G, Z, Y>::UNIFORM) {
     if (ln.left_even)  // warp-uniform branch
       sor_pass<T, G, Z, PHASED, p, SUM, 1>(v, crho, s_cube, ln, omega_6, acc4);
