@@ -403,7 +403,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--one-stream", action="store_true",
                     help="time the step with its batches one after another on one stream")
-    ap.add_argument("--no-extra", action="store_true", help="skip the other configurations (MG, mixed batch, learned guess)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations (MG, mixed batch, learned guess)")
     ap.add_argument("--only", default=None,
                     help="comma list of batches to run (e.g. f64_g5); profiling cases, not a bench line")
     a = ap.parse_args(argv)
@@ -652,13 +653,15 @@ def main(argv=None) -> int:
                    "parallelism": f"patch shards x{world}",
                    "learned_init": "extra.learned_init_sor_g1 (ghost 1, 65536 held-out patches)"},
         "gpu_launches": len(batches) * a.steps,
-        "batches": "one stream" if a.one_stream else "one stream per batch, forked from and joined to the timing stream",
+        "batches": ("one stream" if a.one_stream
+                    else "one stream per batch, forked from and joined to the timing stream"),
         "value_one_stream": value_one_stream,
         "per_batch_ms": {f"f{8 * p.real_size}_g{p.ghost}": float(per_kernel[:, i].mean())
                          for i, (p, _) in enumerate(batches)},
         "mean_iters": {f"f{8 * p.real_size}_g{p.ghost}": float(it.mean()) for (p, _), it in zip(batches, iters)},
         "onchip_frac_per_batch": {
-            f"f{8 * p.real_size}_g{p.ghost}": wavefronts_of(p, it) / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
+            f"f{8 * p.real_size}_g{p.ghost}":
+                wavefronts_of(p, it) / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
             for i, ((p, _), it) in enumerate(zip(batches, iters))},
         "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
