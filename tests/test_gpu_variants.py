@@ -13,7 +13,7 @@ from gpg.inputs import make_patches
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("rs,g", [(4, 1), (4, 3), (8, 2), (8, 3), (8, 5)])
+@pytest.mark.parametrize("rs,g", [(rs, g) for rs in (4, 8) for g in range(1, 6)])
 def test_variants_bit_identical(rs, g):
     torch = pytest.importorskip("torch")
     from gpg.lib import GpgError, check, library, solve_device
