@@ -73,3 +73,24 @@ def test_device_call_without_gpu_reports_error():
     with pytest.raises(GpgError):
         from gpg.lib import set_diagnose_device
         set_diagnose_device(0)
+
+
+def test_sor_variant_table_queries():
+    """The variant table answers without a GPU: 14 launch shapes, each with a
+    CTA size, pass order and layout; out-of-range ids are rejected."""
+    lib = library()
+    n = lib.gpg_sor_variant_count()
+    assert n == 14
+    shapes = set()
+    for v in range(n):
+        ppc, ph, z, y = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib.gpg_sor_variant_info(v, C.byref(ppc), C.byref(ph)))
+        check(lib.gpg_sor_variant_layout(v, C.byref(z), C.byref(y)))
+        assert ppc.value in (1, 2, 4) and ph.value in (0, 1) and z.value in (1, 2) and y.value in (1, 2)
+        shapes.add((ppc.value, ph.value, z.value, y.value))
+    assert len(shapes) == n  # no two variants alike
+    for bad in (-1, n):
+        with pytest.raises(GpgError):
+            check(lib.gpg_sor_variant_layout(bad, None, None))
+    with pytest.raises(GpgError):
+        check(lib.gpg_set_sor_variant(4, 3, n))
