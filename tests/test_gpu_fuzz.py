@@ -4,8 +4,9 @@ oracle (needs a B200).
 Each case draws: scheme (SOR / MG), precision, ghost size 1-5, output ghost
 width 1-2, interpolation (CQUAD / QUAD), 5-point gradient, gravity on or off,
 and per scheme the start (interpolated / zero / caller guess), stopping rule
-(reference growth rule / relative tolerance), omega and iteration limits, or
-the V-cycle count and smoothing sweeps; 1-39 patches.  The comparison is the
+(reference growth rule / relative tolerance), omega and iteration limits and
+the SOR kernel variant (launch shape and lane layout), or the V-cycle count
+and smoothing sweeps; 1-39 patches.  The comparison is the
 one of test_gpu_parity: bit-identical fields wherever the per-patch iteration
 counts agree, counts agreeing for >= 99 % of patches, the rest within the
 relative L-infinity tolerance.
@@ -21,7 +22,7 @@ from test_gpu_parity import compare, gpu_run, torch_cuda  # noqa: F401  (fixture
 
 pytestmark = pytest.mark.gpu
 
-CASES = 32
+CASES = 64
 
 
 def draw(i):
@@ -42,12 +43,15 @@ def draw(i):
     else:
         kw.update(mg_max_iter=int(rng.integers(1, 6)), mg_npre_smooth=int(rng.integers(1, 4)),
                   mg_npost_smooth=int(rng.integers(1, 4)))
-    return scheme, rs, g, kw, int(rng.integers(1, 40)), 9100 + i
+    variant = int(rng.integers(0, 14))
+    return scheme, rs, g, kw, int(rng.integers(1, 40)), 9100 + i, variant
 
 
 @pytest.mark.parametrize("i", range(CASES))
 def test_random_configuration_matches_oracle(torch_cuda, i):
-    scheme, rs, g, kw, npatch, seed = draw(i)
+    import ctypes as C
+    from gpg.lib import GpgError, check, library
+    scheme, rs, g, kw, npatch, seed, variant = draw(i)
     dt = np.float32 if rs == 4 else np.float64
     p = default_params(rs, g, scheme, **kw)
     d = make_patches(npatch, g, seed=seed, gra_ghost=kw["gra_ghost"], dtype=dt, fluid=bool(kw["gra_acc"]))
@@ -57,4 +61,17 @@ def test_random_configuration_matches_oracle(torch_cuda, i):
         guess = (0.01 * np.random.default_rng(seed).standard_normal((npatch, m, m, m))).astype(dt)
     flu = d["flu"].copy() if kw["gra_acc"] else None
     o = run_oracle(p, d["rho"], d["pot_in"], flu=flu, guess=guess, accum_f64=True)
-    compare(p, gpu_run(torch_cuda, p, d, guess=guess), o)
+    lib = library()
+    cur = C.c_int()
+    check(lib.gpg_get_sor_variant(rs, g, C.byref(cur)))
+    check(lib.gpg_set_sor_variant(rs, g, variant))
+    try:
+        out = gpu_run(torch_cuda, p, d, guess=guess)
+    except GpgError as e:
+        assert e.status == 5  # this variant does not fit this configuration
+        out = None
+    finally:
+        check(lib.gpg_set_sor_variant(rs, g, cur.value))
+    if out is None:
+        out = gpu_run(torch_cuda, p, d, guess=guess)
+    compare(p, out, o)
