@@ -698,6 +698,46 @@ extern "C" int gpg_sor_variant_layout(int variant, int *lanes_per_column, int *r
   return GPG_OK;
 }
 
+namespace {
+template <typename T, int G, int Z, int Y>
+void sor_layout_fill(int *o) {
+  using C = gpg::SorCfg<T, G, Z, Y>;
+  const int v[GPG_SOR_LAYOUT_FIELDS] = {Z, Y, C::MH, C::R, C::P, C::PADZ, C::U, C::BLOCK, C::TEAM, C::PP, C::FITS};
+  for (int i = 0; i < GPG_SOR_LAYOUT_FIELDS; ++i) o[i] = v[i];
+}
+
+template <typename T, int G>
+void sor_layout_zy(int z, int y, int *o) {
+  if (z == 1 && y == 1) sor_layout_fill<T, G, 1, 1>(o);
+  else if (z == 2 && y == 1) sor_layout_fill<T, G, 2, 1>(o);
+  else if (z == 2 && y == 2) sor_layout_fill<T, G, 2, 2>(o);
+  else sor_layout_fill<T, G, 1, 2>(o);
+}
+
+template <typename T>
+void sor_layout_g(int g, int z, int y, int *o) {
+  switch (g) {
+    case 1: return sor_layout_zy<T, 1>(z, y, o);
+    case 2: return sor_layout_zy<T, 2>(z, y, o);
+    case 3: return sor_layout_zy<T, 3>(z, y, o);
+    case 4: return sor_layout_zy<T, 4>(z, y, o);
+    default: return sor_layout_zy<T, 5>(z, y, o);
+  }
+}
+}  // namespace
+
+extern "C" int gpg_sor_layout(int real_size, int ghost, int variant, int *fields) {
+  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < 0 || variant >= kSorVariants ||
+      !fields)
+    return fail(GPG_ERR_INVALID, "real_size %d ghost %d variant %d", real_size, ghost, variant);
+  const int z = kSorVariantSplit[variant], y = kSorVariantRows[variant];
+  if (real_size == 4)
+    sor_layout_g<float>(ghost, z, y, fields);
+  else
+    sor_layout_g<double>(ghost, z, y, fields);
+  return GPG_OK;
+}
+
 extern "C" int gpg_set_sor_variant(int real_size, int ghost, int variant) {
   std::call_once(g_tune_once, load_tune_file);
   if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < 0 || variant >= kSorVariants)

@@ -242,6 +242,16 @@ GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
 GPG_API int gpg_sor_variant_count(void);
 GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased);
 GPG_API int gpg_sor_variant_layout(int variant, int *lanes_per_column, int *rows_per_lane);
+/* The lane layout a variant uses at (real_size, ghost), for tools and tests
+ * that check its indexing on the host: fields[GPG_SOR_LAYOUT_FIELDS] =
+ * {lanes per column Z, rows per lane Y, heights per lane MH, lanes per row R,
+ *  row pitch P, plane padding PADZ, block rounding U, lanes per block BLOCK,
+ *  threads per team TEAM, plane pitch PP, built (1) or beyond the register
+ *  file (0)}.  The shared cube of a team is 2 * (8 + 2 ghost) * PP elements;
+ * cell (x, y, z) of colour c = (x + y + z + 1) & 1 sits at
+ * (c * (8 + 2 ghost) + z) * PP + y * P + (x + 1) / 2. */
+#define GPG_SOR_LAYOUT_FIELDS 11
+GPG_API int gpg_sor_layout(int real_size, int ghost, int variant, int *fields);
 GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
 GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
 
