@@ -86,7 +86,9 @@ def tune(npatch=4096, precisions=(4, 8), ghosts=(1, 2, 3, 4, 5)):
             ok = {v: ms for v, ms in times.items() if ms is not None}
             best = min(ok, key=ok.get)
             check(lib.gpg_set_sor_variant(rs, g, best))
-            report[f"f{8 * rs}_g{g}"] = {"best": best, "default": cur.value, "ms": times}
+            report[f"f{8 * rs}_g{g}"] = {"best": best, "default": cur.value, "ms": times,
+                                         "shape": {v: {"patches_per_cta": ppc, "phased": ph, "lanes_per_column": z,
+                                                       "rows_per_lane": y} for v, ppc, ph, z, y in variants()}}
             print(f"f{8 * rs} g{g}: " + "  ".join(f"v{v}={'-' if ms is None else f'{ms:.3f}'}"
                                                  for v, ms in times.items()) + f"  -> v{best}", flush=True)
     return report
