@@ -47,8 +47,15 @@ int fail(int status, const char *fmt, ...) {
 // ---------------------------------------------------------------------------
 // launch configuration per (precision, ghost size)
 // ---------------------------------------------------------------------------
-// MG threads per CTA (one patch per CTA).
-template <int G> constexpr int mg_threads() { return G <= 2 ? 128 : 256; }
+// MG threads per CTA (one patch per CTA).  FP32, measured on B200 (ghost 3 with
+// 5-point gravity, 16384 patches: 128 threads 0.918 ms, 256 0.957, 512 1.065;
+// ghost 5: 512 threads 0.522 ms, 256 0.542, 128 0.606; ghost 4: 256 best);
+// FP64 keeps 128 up to ghost 2 and 256 above.  Results do not depend on it.
+template <typename T, int G>
+constexpr int mg_threads() {
+  if constexpr (sizeof(T) == 4) return G <= 3 ? 128 : (G == 4 ? 256 : 512);
+  return G <= 2 ? 128 : 256;
+}
 
 // Kernel attributes, set once per kernel instantiation (the caller owns the
 // flag): the dynamic shared memory size and the max-shared carveout (the
@@ -222,7 +229,7 @@ int prepare_solve_kernels(const gpg_params &q) {
 
 template <typename T, int G>
 int launch_mg(const gpg::SolveArgs<T> &a, cudaStream_t s) {
-  constexpr int NT = mg_threads<G>();
+  constexpr int NT = mg_threads<T, G>();
   const size_t smem = gpg::MgSmem<T, G, NT>::bytes;
   auto fn = gpg::mg_kernel<T, G, NT>;
   static AttrOnce attr;
