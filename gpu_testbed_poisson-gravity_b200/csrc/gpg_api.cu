@@ -47,14 +47,16 @@ int fail(int status, const char *fmt, ...) {
 // ---------------------------------------------------------------------------
 // launch configuration per (precision, ghost size)
 // ---------------------------------------------------------------------------
-// MG threads per CTA (one patch per CTA).  FP32, measured on B200 (ghost 3 with
-// 5-point gravity, 16384 patches: 128 threads 0.918 ms, 256 0.957, 512 1.065;
-// ghost 5: 512 threads 0.522 ms, 256 0.542, 128 0.606; ghost 4: 256 best);
-// FP64 keeps 128 up to ghost 2 and 256 above.  Results do not depend on it.
+// MG threads per CTA (one patch per CTA), from a B200 sweep of 128-1024
+// threads per (precision, ghost size); results do not depend on it.  FP32:
+// ghost 3 with 5-point gravity, 16384 patches: 128 threads 0.918 ms, 256 0.957,
+// 512 1.065; ghost 5: 512 threads 0.522 ms, 256 0.542, 128 0.606; ghost 4: 256.
+// FP64 (about 160 registers per thread): ghost 3, 2048 patches: 128 threads
+// 1.228 ms, 256 1.366; ghost 4 and 5: 256 (512 and 1024 spill); ghost 1-2: 128.
 template <typename T, int G>
 constexpr int mg_threads() {
   if constexpr (sizeof(T) == 4) return G <= 3 ? 128 : (G == 4 ? 256 : 512);
-  return G <= 2 ? 128 : 256;
+  return G <= 3 ? 128 : 256;
 }
 
 // Kernel attributes, set once per kernel instantiation (the caller owns the
