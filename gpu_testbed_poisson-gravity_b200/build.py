@@ -9,6 +9,7 @@ _build/ptxas_libgpg.log at the repository root.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -47,20 +48,36 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
+def _compile(src: str, obj: str):
+    cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", "-o", obj, src]
+    return cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every csrc/*.cu to an object (in parallel), then link libgpg.so."""
     if not force and up_to_date():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(BUILD_LOG_DIR, exist_ok=True)
-    cmd = ([nvcc()] + ARCH + NVCC_FLAGS + ["-shared", "-o", LIB] + sources()
-           + ["-lcudart"])
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    objs = [os.path.join(BUILD_LOG_DIR, os.path.basename(s)[:-3] + ".o") for s in sources()]
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(objs)) as ex:
+        results = list(ex.map(_compile, sources(), objs))
+    log = ""
+    for cmd, r in results:
+        if verbose:
+            print(" ".join(cmd))
+        log += r.stdout + r.stderr
     with open(os.path.join(BUILD_LOG_DIR, "ptxas_libgpg.log"), "w") as f:
-        f.write(r.stdout + r.stderr)
+        f.write(log)
+    for cmd, r in results:
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stderr[-6000:])
+    link = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if verbose:
+        print(" ".join(link))
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stderr[-6000:])
+        raise RuntimeError("link failed:\n" + r.stderr[-6000:])
     return LIB
 
 

@@ -21,6 +21,7 @@
 #include "convnet_kernels.cuh"
 #include "convnet_infer.cuh"
 #include "interp.cuh"
+#include "optim.cuh"
 
 using gpg::net::ConvArgs;
 using gpg::net::WgradArgs;
@@ -208,19 +209,6 @@ __global__ void reduce_grad_kernel(const float *__restrict__ wpart, int nwpart, 
   }
 }
 
-__global__ void adam_kernel(float *__restrict__ p, float *__restrict__ m, float *__restrict__ v,
-                            const float *__restrict__ g, int64_t n, float lr, float b1, float b2, float eps,
-                            float c1, float c2) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.f - b1) * gi;
-    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-  }
-}
-
 // pack W[27][cin][cout] (FP32) into the forward operand [KCH][cout][8] (bf16,
 // k = tap*cin + c) and, when bwd != nullptr, the backward-data operand
 // [KCH'][cin][8] with k' = tap'*cout + n and W'[tap'][n][c] = W[26-tap'][c][n]
@@ -241,39 +229,57 @@ __global__ void pack_kernel(const float *__restrict__ w, int cin, int cout, int 
   }
 }
 
+// kernel attributes belong to a device's context: set once per (kernel, device)
+constexpr int kMaxDevices = 64;
+struct DevOnce {
+  std::once_flag once[kMaxDevices];
+  cudaError_t err[kMaxDevices] = {};
+};
+
+int device_index() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+  return dev;
+}
+
 template <typename F>
-int set_attr_once(F *fn, size_t bytes, std::once_flag &once, cudaError_t &err) {
-  std::call_once(once, [&] {
+int set_attr_once(F *fn, size_t bytes, DevOnce &st) {
+  const int dev = device_index();
+  if (dev < 0) return nfail(GPG_ERR_UNSUPPORTED, "current device out of range");
+  std::call_once(st.once[dev], [&] {
+    cudaError_t &err = st.err[dev];
     err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
   });
-  if (err != cudaSuccess) return nfail(GPG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(err));
+  if (st.err[dev] != cudaSuccess)
+    return nfail(GPG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st.err[dev]));
   return GPG_OK;
 }
 
 // blocks of the bias-gradient and loss kernels = partial sums they leave
 constexpr int kPartials = 148;
 
+// SM count of the current device (cached per device)
 int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
+  static int n[kMaxDevices] = {};
+  const int dev = device_index();
+  if (dev < 0) return 148;
+  if (!n[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    n[dev] = v > 0 ? v : 148;
   }
-  return n;
+  return n[dev];
 }
 
 template <int CIN, int NOUT, int EPI>
 int launch_conv(const ConvArgs &a, cudaStream_t s) {
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
+  static DevOnce once;
   constexpr size_t smem = gpg::net::ConvSmem<CIN, NOUT>::bytes;
   auto fn = gpg::net::conv_fwd_kernel<CIN, NOUT, EPI>;
-  if (int rc = set_attr_once(fn, smem, once, err)) return rc;
+  if (int rc = set_attr_once(fn, smem, once)) return rc;
   const int64_t ntile = (a.M + 127) / 128;
   // at most 512/32 TMEM column blocks per SM; shared memory bounds it earlier
   const int64_t grid = std::min<int64_t>(ntile, int64_t(sm_count()) * 4);
@@ -293,14 +299,13 @@ int wgrad_grid(int64_t M) {
 template <int CIN, int NOUT>
 int launch_wgrad(const WgradArgs &a, int grid, cudaStream_t s) {
   using W = gpg::net::WgradCfg<CIN, NOUT>;
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
+  static DevOnce once;
   // shared memory sized so that the CTAs an SM holds never ask for more than
   // its 512 TMEM columns in total
   const int per_sm = 512 / W::COLS;
   const size_t smem = std::max<size_t>(W::bytes, per_sm >= 6 ? W::bytes : (220 * 1024) / per_sm);
   auto fn = gpg::net::conv_wgrad_kernel<CIN, NOUT>;
-  if (int rc = set_attr_once(fn, smem, once, err)) return rc;
+  if (int rc = set_attr_once(fn, smem, once)) return rc;
   if (grid <= 0) return GPG_OK;
   fn<<<(unsigned)grid, 128, smem, s>>>(a);
   NET_CUDA(cudaGetLastError());
@@ -571,10 +576,9 @@ extern "C" int gpg_net_predict(gpg_net *n, int npatch, const float *d_rho, const
   if (npatch && (!d_rho || !d_pot_in || !d_guess)) return nfail(GPG_ERR_INVALID, "NULL array");
   if (!npatch) return GPG_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
+  static DevOnce once;
   using gpg::net::InferSmem;
-  if (int rc = set_attr_once(gpg::net::net_infer_kernel, InferSmem::bytes, once, err)) return rc;
+  if (int rc = set_attr_once(gpg::net::net_infer_kernel, InferSmem::bytes, once)) return rc;
   gpg::net::InferArgs a{};
   a.rho = d_rho;
   a.pot_in = d_pot_in;
@@ -625,7 +629,7 @@ int adam_step(gpg_net *n, const float *grad, float lr, cudaStream_t s) {
   n->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - std::pow(b1, float(n->step)), c2 = 1.f - std::pow(b2, float(n->step));
-  adam_kernel<<<128, 256, 0, s>>>(n->params, n->adam_m, n->adam_v, grad, kParams, lr, b1, b2, 1e-8f, c1, c2);
+  gpg::adam_kernel<<<128, 256, 0, s>>>(n->params, n->adam_m, n->adam_v, grad, kParams, lr, b1, b2, 1e-8f, c1, c2);
   NET_CUDA(cudaGetLastError());
   return repack(n, s);
 }

@@ -9,7 +9,8 @@
 //        phi += Omega/6 R,   Total += |R|      (Total accumulated in double)
 //      stop after the first sweep whose Total grows once Iter+1 >= Min_Iter
 //      (or, in tolerance mode, once Total <= tol * sum|Const rho| -- or <= tol
-//      in absolute-tolerance mode); cap Max_Iter
+//      in absolute-tolerance mode, or <= tol * sum|phi_interp| over the
+//      updated cells in potential-tolerance mode); cap Max_Iter
 //   c. copy the GRA_NXT^3 window of the cube to pot_out
 //
 // B200 layout.  A team of 1-8 warps owns a patch.  A lane owns the interior
@@ -323,13 +324,30 @@ __device__ __forceinline__ void sor_pass_any(T (&v)[Y][2][SorCfg<T, G, Z, Y>::MH
   }
 }
 
+// What a start-value hook sees: the lane's columns (v) and Const*rho (crho)
+// in registers, the team's shared cube and the lane's place in it.
+template <typename T, int G, int Z, int Y>
+struct SorLaneState {
+  using C = SorCfg<T, G, Z, Y>;
+  T (&v)[Y][2][C::MH + 2];
+  const T (&crho)[Y][2][C::MH];
+  T *s_cube;
+  const SorLane &ln;
+  bool active;  // the lane owns cells
+  int y, h, zbase;
+};
+
 // Solve patch P_ with the team `team` (thread `tid` of TEAM) whose shared
 // memory starts at `tb` (SorSmem::team_bytes).  Used by the per-ghost-size
 // kernel below and by the mixed-size persistent kernel (batch_kernel.cuh),
-// so both produce the same bits for a patch.
-template <typename T, int G, bool PHASED, int Z = 1, int Y = 1>
-__device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P_, int team, int tid,
-                                                unsigned char *tb) {
+// so both produce the same bits for a patch.  `hook(state)` runs once the
+// start values and the stopping bound are set, before the first sweep; it
+// may change the interior (registers and shared cube) and must leave the
+// team synchronised.  store == false skips every global write (a team that
+// only keeps a CTA-wide schedule going).
+template <typename T, int G, bool PHASED, int Z, int Y, typename Hook>
+__device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int64_t P_, int team, int tid,
+                                                     unsigned char *tb, bool store, Hook &&hook) {
   using g = Geo<G>;
   using C = SorCfg<T, G, Z, Y>;
   using S = SorSmem<T, G, Z, Y>;
@@ -386,7 +404,9 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
           const int x = left ? 2 * h + 1 : 2 * h + 2;
           const int idx = ((z - 1) * M + (yr - 1)) * M + (x - 1);
           crho[rr][c][zz - 1] = active ? mul(a.sor_const, __ldg(rho + idx)) : T(0);
-          cr_sum += (double)absval(crho[rr][c][zz - 1]);
+          // tolerance scale: sum |Const rho| (mode 1) or sum |interpolated
+          // phi| over the updated cells, before a start mode replaces it (3)
+          cr_sum += (double)absval(a.stop_mode == 3 ? (active ? v[rr][c][zz] : T(0)) : crho[rr][c][zz - 1]);
           if (a.init_mode != 0) v[rr][c][zz] = (a.init_mode == 2 && active) ? __ldg(guess + idx) : T(0);
         }
       }
@@ -402,7 +422,7 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
         for (int zz = 1; zz <= MH; ++zz) s_cube[(c * N + zbase + zz) * PP + ln.own + rr * P] = v[rr][c][zz];
   }
   double tol_abs = 0.0;
-  if (a.stop_mode == 1) {
+  if (a.stop_mode == 1 || a.stop_mode == 3) {
     cr_sum = warp_sum(cr_sum);
     if constexpr (NWARP > 1) {
       if (lane == 0) s_part[warp] = cr_sum;
@@ -418,6 +438,7 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
     tol_abs = a.sor_tol;
   }
   team_sync<TEAM>(team);
+  hook(SorLaneState<T, G, Z, Y>{v, crho, s_cube, ln, active, y, h, zbase});
 
   // ---- SOR sweeps ---------------------------------------------------------
   const T omega_6 = a.omega_6;
@@ -464,6 +485,7 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
     }
     total_old = total;
   }
+  if (!store) return;
   if (tid == 0) {
     if (a.iters) a.iters[P_] = iter;
     if (a.resid) a.resid[P_] = last;
@@ -483,6 +505,12 @@ __device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P
     gravity_patch<T, TEAM>(a.flu + P_ * 5 * 512, tid, a.gra_const, a.p5,
                            [s_cube](int i, int j, int k) { return s_cube[C::addr(i + G, j + G, k + G)]; });
   }
+}
+
+template <typename T, int G, bool PHASED, int Z = 1, int Y = 1>
+__device__ __forceinline__ void sor_solve_patch(const SolveArgs<T> &a, int64_t P_, int team, int tid,
+                                                unsigned char *tb) {
+  sor_solve_patch_with<T, G, PHASED, Z, Y>(a, P_, team, tid, tb, true, [](const auto &) {});
 }
 
 // PPC: teams (patches) per CTA.  PHASED: form the MH independent updates of a

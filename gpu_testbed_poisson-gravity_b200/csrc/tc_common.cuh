@@ -105,17 +105,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait for phase `parity`: gives up after about one second (or 2^26
-// polls); returns false (and sets *err) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+// Bounded wait for phase `parity`: gives up after `max_polls` polls or about
+// one second, whichever comes first; returns false (and sets *err) on timeout.
+__device__ __forceinline__ bool mbar_wait_polls(uint64_t *bar, uint32_t parity, int *err, uint32_t max_polls) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  for (uint32_t i = 1; i < (1u << 26); ++i) {
+  for (uint32_t i = 1; i < max_polls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 255u) == 0u && globaltimer_ns() - t0 > 1000000000ull) break;
   }
   if (err) atomicExch(err, 1);
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+  return mbar_wait_polls(bar, parity, err, 1u << 26);
 }
 
 // --- TMEM -> registers: 32 lanes x 16 columns of 32-bit per warp -----------

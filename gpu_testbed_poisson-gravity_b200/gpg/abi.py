@@ -15,7 +15,7 @@ GPG_ERR_STATE = 6
 GPG_SOR, GPG_MG = 1, 2
 GPG_INT_CQUAD, GPG_INT_QUAD = 4, 5
 GPG_INIT_INTERP, GPG_INIT_ZERO, GPG_INIT_GUESS = 0, 1, 2
-GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE, GPG_STOP_ABS_TOLERANCE = 0, 1, 2
+GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE, GPG_STOP_ABS_TOLERANCE, GPG_STOP_POT_TOLERANCE = 0, 1, 2, 3
 NULL_INT = 2147483647
 
 
@@ -84,6 +84,14 @@ class GpgBatchGroup(C.Structure):
 
 SOR_OMEGA = {1: 1.49, 2: 1.57, 3: 1.62, 4: 1.65, 5: 1.69}
 
+# The fixed residual of GPG_STOP_POT_TOLERANCE per (sizeof(real), ghost):
+# 2 x the 90th percentile of L1 residual / sum|interpolated phi| at the
+# reference stopping point (CPU_PoissonSolver_SOR.cpp:275-281) of zero-start
+# SOR on the seeded power-law inputs (oracle/calibrate_tol.py, 1024 patches,
+# seed 11); gpg_pot_tolerance() in the C library returns the same values.
+POT_TOL = {(4, 1): 9.8e-7, (4, 2): 1.1e-6, (4, 3): 1.2e-6, (4, 4): 1.3e-6, (4, 5): 1.4e-6,
+           (8, 1): 1.8e-15, (8, 2): 2.1e-15, (8, 3): 2.3e-15, (8, 4): 2.4e-15, (8, 5): 2.5e-15}
+
 
 def default_params(real_size: int = 4, ghost: int = 1, scheme: int = GPG_SOR, **kw) -> GpgParams:
     """Reference defaults (Main.cpp:1142-1223, Makefile:41-48) in Python;
@@ -125,3 +133,15 @@ def patch_sizes(p: GpgParams) -> dict:
     gn = 8 + 2 * G
     return {"rho": m ** 3, "pot_in": pn ** 3, "pot_out": gn ** 3, "flu": 5 * 512,
             "rho_nxt": m, "pot_nxt": pn, "gra_nxt": gn, "cube": 8 + 2 * g}
+
+
+def fixed_residual_params(real_size: int, ghost: int, init_mode: int = GPG_INIT_ZERO, max_iter: int = 300,
+                          **kw) -> GpgParams:
+    """SOR to the calibrated fixed residual: stop at the first sweep whose L1
+    residual is <= POT_TOL x sum|interpolated phi| (Min_Iter 1, Max_Iter
+    `max_iter`), Poisson only, interior output (gra_ghost 0)."""
+    d = dict(gra_acc=0, gra_ghost=0, init_mode=init_mode, stop_mode=GPG_STOP_POT_TOLERANCE,
+             sor_tolerance=POT_TOL[(real_size, ghost)], sor_min_iter=1, sor_max_iter=max_iter)
+    d.update(kw)
+    return default_params(real_size, ghost, GPG_SOR, **d)
+

@@ -48,6 +48,7 @@ def library(path: str | None = None):
         "gpg_last_error": (C.c_char_p, []),
         "gpg_default_params": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
         "gpg_validate_params": (C.c_int, [P]),
+        "gpg_pot_tolerance": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
         "gpg_patch_sizes": (C.c_int, [P] + [C.POINTER(C.c_int64)] * 4),
         "gpg_poisson_gravity_device": (C.c_int, [P, C.c_int] + [vp] * 8),
         "gpg_set_diagnose_device": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),

@@ -1,21 +1,31 @@
-"""Train and evaluate the learned initial guess for ghost-size-1 SOR.
+"""Train and evaluate the learned initial guesses for ghost-size-1 SOR.
 
-    python gpu_testbed_poisson-gravity_b200/learned.py train --npatch 1048576 --epochs 2 \
+    python gpu_testbed_poisson-gravity_b200/learned.py train --model lin --npatch 1048576 \
+        --out gpu_testbed_poisson-gravity_b200/weights/lin_correction
+    python gpu_testbed_poisson-gravity_b200/learned.py train --model conv --npatch 1048576 --epochs 2 \
         --out gpu_testbed_poisson-gravity_b200/weights/learned_init
-    python gpu_testbed_poisson-gravity_b200/learned.py eval  --npatch 65536 \
-        --weights gpu_testbed_poisson-gravity_b200/weights/learned_init
+    python gpu_testbed_poisson-gravity_b200/learned.py eval --npatch 65536
+
+Two models, both trained on the GPU by the library's own kernels:
+
+* ``lin`` (gpg_lin_*): a learned linear correction of the interpolated start,
+  equivariant under the cube's reflections (4 class matrices of 64 x 64 over
+  the parity blocks of the residual of that start), fused into the SOR kernel
+  and applied on the tensor cores (65,536 FLOP per patch);
+* ``conv`` (gpg_net_*): the 4-layer 3^3 convolution network (8 -> 32 -> 32 ->
+  32 -> 16 channels) that maps density and boundary shell to the interior
+  (116.7 MFLOP per patch).
 
 Data: seeded ghost-1 patches (gpg.inputs) with rho0 log-uniform over 4
 decades and power index uniform in [1.5, 2.5].  Targets are the plain SOR's own
 solutions (reference rule from the interpolated start, i.e. converged to the
-FP32 round-off floor) computed by libgpg.  Training and inference run on the
-library's tensor-core kernels (gpg_net_*).  Evaluation solves held-out patches
-(other seeds) from a zero start and from the learned guess to the same
-relative tolerance and reports sweeps, patches/s (the network's inference
-included) and the error against an FP64 solution of the same patches.
-Weights are saved as <out>.bin (float32) with a <out>.json header;
-weights/learned_init.* is the checkpoint of the command above (2^20 patches,
-seed 1, 2 epochs of batch 1024, Adam with a cosine learning-rate schedule).
+FP32 round-off floor) computed by libgpg.  Evaluation solves held-out patches
+(other seeds) to the calibrated fixed residual (GPG_STOP_POT_TOLERANCE,
+gpg.abi.POT_TOL) from a zero start, from the interpolated start and from each
+learned start, and reports sweeps, patches/s (the model's cost included) and
+the error against an FP64 solution of the same patches.  Weights are saved as
+<out>.bin (float32) with a <out>.json header; weights/lin_correction.* and
+weights/learned_init.* are the checkpoints of the commands above.
 """
 from __future__ import annotations
 
@@ -31,12 +41,18 @@ sys.path.insert(0, HERE)
 import numpy as np  # noqa: E402
 
 from gpg.abi import (GPG_INIT_GUESS, GPG_INIT_INTERP, GPG_INIT_ZERO, GPG_SOR,  # noqa: E402
-                     GPG_STOP_TOLERANCE, default_params)
+                     POT_TOL, default_params, fixed_residual_params)
 from gpg.inputs import log_uniform, make_patches  # noqa: E402
 
 CNST = float(np.float32(np.float32(4 * np.pi * 1e-5) * np.float32(1.0) * np.float32(1.0)))
 CHUNK = 65536
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "learned_init")
+DEFAULT_LIN = os.path.join(HERE, "weights", "lin_correction")
+# learned linear correction per patch: 8 blocks x 64 x 64 multiply-adds
+# (algorithmic) and 16 MMAs of 128 x 16 x 16 per 8 patches (executed: the two
+# blocks of an MMA also meet each other's matrix)
+LIN_FLOP = 8 * 2 * 64 * 64
+LIN_FLOP_EXECUTED = 16 * 2 * 128 * 16 * 16 // 8
 # algorithmic FLOPs of one patch's forward pass: 3^3 convolutions 3 -> 32 -> 32
 # -> 32 on the 10^3 cube, 32 -> 1 on the 8^3 interior
 NET_FLOP = 2 * 27 * (1000 * (3 * 32 + 32 * 32 + 32 * 32) + 512 * 32)
@@ -78,10 +94,9 @@ def shard(n: int, rank: int, world: int) -> tuple[int, int]:
     return lo * CHUNK, min(hi * CHUNK, n)
 
 
-def sor_params(real_size: int, init_mode: int, stop_mode: int = GPG_STOP_TOLERANCE, tol: float = 0.02,
-               max_iter: int = 300):
-    return default_params(real_size, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=init_mode, stop_mode=stop_mode,
-                          sor_tolerance=tol, sor_min_iter=1, sor_max_iter=max_iter)
+def sor_params(real_size: int, init_mode: int, max_iter: int = 300):
+    """SOR to the calibrated fixed residual (Min_Iter 1, Poisson only)."""
+    return fixed_residual_params(real_size, 1, init_mode=init_mode, max_iter=max_iter)
 
 
 def solve(torch, p, rho, pin, guess=None):
@@ -198,70 +213,182 @@ def _event_ms(torch, fn, reps=3):
     return s.elapsed_time(e) / reps
 
 
-def evaluate(net, npatch: int, seed: int, tol: float = 0.02):
-    """Zero-start plain SOR vs learned-guess SOR to the same relative tolerance
-    (and the reference's interpolated start beside them), then all three
-    starts under the reference's own stopping rule."""
+def _stats(it):
+    a = it.cpu().numpy()
+    return {"mean": float(a.mean()), "p50": float(np.median(a)), "p90": float(np.percentile(a, 90)),
+            "max": int(a.max())}
+
+
+def evaluate(net=None, lin=None, npatch: int = 65536, seed: int = 99, reps: int = 5, rule: bool = True):
+    """Every start solved to the same calibrated fixed residual (FP32,
+    GPG_STOP_POT_TOLERANCE, Min_Iter 1, Max_Iter 300): zero interior (the
+    plain SOR the metric compares against), the reference's interpolated
+    start, the learned linear correction (`lin`, fused into the SOR kernel)
+    and the convolution network's guess (`net`, a separate inference kernel
+    ahead of the SOR).  Times are CUDA-event means over `reps` launches after a
+    warm-up, the model's own cost included.  With `rule`, the same starts
+    under the reference's own stopping rule as well."""
     import torch
     dev = torch.device("cuda:0")
     rho_h, pin_h = dataset(npatch, seed)
     rho, pin = torch.from_numpy(rho_h).to(dev), torch.from_numpy(pin_h).to(dev)
-    p0 = sor_params(4, GPG_INIT_ZERO, tol=tol)
-    pg = sor_params(4, GPG_INIT_GUESS, tol=tol)
-    guess = torch.empty((npatch, 8, 8, 8), device=dev)
-    out = {}
-    ms_plain = _event_ms(torch, lambda: solve(torch, p0, rho, pin))
-    pot0, it0, _ = solve(torch, p0, rho, pin)
-    ms_net = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST))
-    ms_net_layers = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST, fused=False))
-    net.predict(rho, pin, guess, CNST)
-    ms_sor_g = _event_ms(torch, lambda: solve(torch, pg, rho, pin, guess=guess))
-    potg, itg, _ = solve(torch, pg, rho, pin, guess=guess)
-    net.check()
-    # FP64 solution of the same patches: reference rule from the interpolated start
+    # FP64 solution of the same patches: reference rule, interpolated start
     p64 = default_params(8, 1, GPG_SOR, gra_acc=0, gra_ghost=0)
     pot64, _, _ = solve(torch, p64, rho.double(), pin.double())
     ref = pot64.cpu().numpy().reshape(npatch, -1)
+    scale = np.abs(ref).max(1)
 
     def err(pot):
         a = pot.double().cpu().numpy().reshape(npatch, -1)
-        return float((np.abs(a - ref).max(1) / np.abs(ref).max(1)).max())
+        e = np.abs(a - ref).max(1) / scale
+        return {"max": float(e.max()), "p50": float(np.median(e))}
 
-    def stats(it):
-        a = it.cpu().numpy()
-        return {"mean": float(a.mean()), "p50": float(np.median(a)), "p90": float(np.percentile(a, 90)),
-                "max": int(a.max())}
+    out = {"workload": f"{npatch} held-out ghost-1 patches (seed {seed}), FP32",
+           "tolerance": (f"L1 residual <= {POT_TOL[(4, 1)]} x sum|interpolated phi| over the updated cells "
+                         "(calibrated fixed residual, GPG_STOP_POT_TOLERANCE), Min_Iter 1, Max_Iter 300")}
+    guess = torch.empty((npatch, 8, 8, 8), device=dev) if net is not None else None
 
-    out["tolerance"] = f"L1 residual <= {tol} x L1 source norm, Min_Iter 1, Max_Iter 300, FP32"
-    out["plain_zero_start"] = {"sweeps": stats(it0), "ms": ms_plain, "patches_per_s": npatch / ms_plain * 1e3,
-                               "rel_linf_vs_fp64": err(pot0)}
-    out["learned_init"] = {"sweeps": stats(itg), "ms_network": ms_net, "ms_network_per_layer_kernels": ms_net_layers,
-                           "network_tflops": NET_FLOP * npatch / ms_net * 1e-9, "ms_sor": ms_sor_g,
-                           "ms": ms_net + ms_sor_g, "patches_per_s": npatch / (ms_net + ms_sor_g) * 1e3,
-                           "rel_linf_vs_fp64": err(potg)}
-    pi = sor_params(4, GPG_INIT_INTERP, tol=tol)
-    ms_interp = _event_ms(torch, lambda: solve(torch, pi, rho, pin))
-    poti, iti, _ = solve(torch, pi, rho, pin)
-    out["plain_interpolated_start"] = {"sweeps": stats(iti), "ms": ms_interp,
-                                       "patches_per_s": npatch / ms_interp * 1e3, "rel_linf_vs_fp64": err(poti)}
-    g = guess.double().cpu().numpy().reshape(npatch, -1)
-    out["learned_init"]["guess_rel_linf_vs_fp64"] = float((np.abs(g - ref).max(1) / np.abs(ref).max(1)).mean())
-    out["speedup_vs_plain"] = ms_plain / (ms_net + ms_sor_g)
-    out["sweep_ratio"] = out["plain_zero_start"]["sweeps"]["mean"] / max(1e-9, out["learned_init"]["sweeps"]["mean"])
-    # the reference's own criterion (Min_Iter 10, stop when the L1 residual
-    # grows, Max_Iter 60) from its interpolated start, a zero start and the guess
-    rr = {"criterion": "reference rule: Min_Iter 10, stop at the first growth of the L1 residual, Max_Iter 60, FP32"}
-    for name, mode in (("interpolated_start", GPG_INIT_INTERP), ("zero_start", GPG_INIT_ZERO),
-                       ("learned_start", GPG_INIT_GUESS)):
-        pr = default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=mode)
-        gg = guess if mode == GPG_INIT_GUESS else None
-        ms = _event_ms(torch, lambda: solve(torch, pr, rho, pin, guess=gg))
-        pot, it, _ = solve(torch, pr, rho, pin, guess=gg)
-        tot = ms + (ms_net if mode == GPG_INIT_GUESS else 0.0)
-        rr[name] = {"sweeps": stats(it), "ms": tot, "patches_per_s": npatch / tot * 1e3,
-                    "rel_linf_vs_fp64": err(pot)}
-    out["reference_rule"] = rr
+    def arm(p, start: str, **kw):
+        if start == "lin":
+            fn = lambda: lin.solve(p, rho, pin)  # noqa: E731
+        elif start == "conv":
+            def fn():
+                net.predict(rho, pin, guess, CNST)
+                return solve(torch, p, rho, pin, guess=guess)
+        else:
+            fn = lambda: solve(torch, p, rho, pin)  # noqa: E731
+        ms = _event_ms(torch, fn, reps)
+        res = fn()
+        pot, it = res[0], res[2] if start == "lin" else res[1]
+        rec = {"sweeps": _stats(it), "ms": ms, "patches_per_s": npatch / ms * 1e3, "rel_linf_vs_fp64": err(pot)}
+        rec.update(kw)
+        return rec
+
+    out["plain_zero_start"] = arm(sor_params(4, GPG_INIT_ZERO), "plain")
+    out["plain_interpolated_start"] = arm(sor_params(4, GPG_INIT_INTERP), "plain")
+    if lin is not None:
+        out["learned_linear"] = arm(sor_params(4, GPG_INIT_INTERP), "lin", model="linear correction",
+                                    flop_per_patch=LIN_FLOP, flop_per_patch_executed=LIN_FLOP_EXECUTED)
+        lin.check()
+    if net is not None:
+        ms_net = _event_ms(torch, lambda: net.predict(rho, pin, guess, CNST), reps)
+        out["learned_conv"] = arm(sor_params(4, GPG_INIT_GUESS), "conv", model="conv net", ms_network=ms_net,
+                                  network_tflops=NET_FLOP * npatch / ms_net * 1e-9, flop_per_patch=NET_FLOP,
+                                  flop_per_patch_executed=NET_FLOP_EXECUTED)
+        net.check()
+    z = out["plain_zero_start"]["ms"]
+    for k in ("plain_interpolated_start", "learned_linear", "learned_conv"):
+        if k in out:
+            out[k]["speedup_vs_zero_start"] = z / out[k]["ms"]
+    if lin is not None:
+        out["learned_linear"]["speedup_vs_interpolated_start"] = (out["plain_interpolated_start"]["ms"] /
+                                                                  out["learned_linear"]["ms"])
+    if rule:
+        rr = {"criterion": "reference rule: Min_Iter 10, stop at the first growth of the L1 residual, Max_Iter 60"}
+        pr = lambda mode: default_params(4, 1, GPG_SOR, gra_acc=0, gra_ghost=0, init_mode=mode)  # noqa: E731
+        rr["zero_start"] = arm(pr(GPG_INIT_ZERO), "plain")
+        rr["interpolated_start"] = arm(pr(GPG_INIT_INTERP), "plain")
+        if lin is not None:
+            rr["learned_linear"] = arm(pr(GPG_INIT_INTERP), "lin")
+        if net is not None:
+            rr["learned_conv"] = arm(pr(GPG_INIT_GUESS), "conv")
+        out["reference_rule"] = rr
     return out
+
+
+def lin_data(lin, rho, pin, chunk: int = CHUNK):
+    """Training features (u, t) of ghost-1 patches: the folded residual of the
+    interpolated start and the folded correction to the plain SOR's solution."""
+    import torch
+    n = rho.shape[0]
+    u = torch.empty((n, 8, 64), device=rho.device)
+    t = torch.empty((n, 8, 64), device=rho.device)
+    p = sor_params(4, GPG_INIT_INTERP)
+    for c0 in range(0, n, chunk):
+        sl = slice(c0, min(n, c0 + chunk))
+        tg = targets(torch, rho[sl], pin[sl])
+        uu, tt = lin.features(p, rho[sl], pin[sl], target=tg)
+        u[sl], t[sl] = uu, tt
+    return u, t
+
+
+def train_lin(npatch: int, epochs: int, batch: int, lr: float, seed: int, out: str | None, log=print):
+    """Train the linear correction on npatch patches with global batch `batch`
+    (Adam, cosine learning rate, parameters from zero).  Under torchrun the
+    step is data-parallel as in train(): per-rank gradients of batch / world
+    patches, averaged with an all-reduce, the same Adam step everywhere."""
+    import torch
+    import torch.distributed as dist
+    from gpg.linear import LinearGuess
+    from gpg.shard import allreduce_mean_
+    distributed = "RANK" in os.environ and "WORLD_SIZE" in os.environ
+    rank, world = (int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])) if distributed else (0, 1)
+    if distributed and not dist.is_initialized():
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if batch % world:
+        raise ValueError(f"global batch {batch} is not a multiple of {world} ranks")
+    lb = batch // world
+    t0 = time.time()
+    first, stop = shard(npatch, rank, world)
+    rho_h, pin_h = dataset(npatch, seed, first=first, stop=stop)
+    lin = LinearGuess(max_batch=lb)
+    u, t = lin_data(lin, torch.from_numpy(rho_h).to(dev), torch.from_numpy(pin_h).to(dev))
+    del rho_h, pin_h
+    torch.cuda.synchronize()
+    t_data = time.time() - t0
+    nb = (stop - first) // lb
+    if distributed:
+        tn = torch.tensor([nb], device=dev)
+        dist.all_reduce(tn, op=dist.ReduceOp.MIN)
+        nb = int(tn.item())
+    loss = torch.empty(1, device=dev)
+    grad = torch.empty(lin.nparams, device=dev) if distributed else None
+    nstep = epochs * nb
+    g = torch.Generator(device="cpu").manual_seed(seed + 7919 * rank)
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hist = []
+    s_ev.record()
+    step = 0
+    for ep in range(epochs):
+        perm = torch.randperm(nb, generator=g)
+        for bi in perm.tolist():
+            sl = slice(bi * lb, (bi + 1) * lb)
+            cur_lr = float(lr * 0.5 * (1 + np.cos(np.pi * step / max(1, nstep))))
+            if distributed:
+                lin.gradients(u[sl], t[sl], grad=grad, loss=loss)
+                allreduce_mean_(grad)
+                lin.apply_gradient(grad, cur_lr)
+            else:
+                lin.train_step(u[sl], t[sl], cur_lr, loss=loss)
+            step += 1
+            if step % 256 == 0 or step == nstep:
+                if distributed:
+                    allreduce_mean_(loss)
+                hist.append((step, float(loss.item())))
+                if rank == 0:
+                    log(f"step {step}/{nstep} loss {hist[-1][1]:.4e}")
+    e_ev.record()
+    torch.cuda.synchronize()
+    ms = s_ev.elapsed_time(e_ev)
+    meta = {"model": "linear correction", "npatch": npatch, "epochs": epochs, "batch": batch, "lr": lr,
+            "seed": seed, "steps": nstep, "ranks": world, "train_ms": ms, "ms_per_step": ms / max(1, nstep),
+            "data_s": t_data, "loss_history": hist}
+    if out and rank == 0:
+        flat = lin.params()
+        flat.tofile(out + ".bin")
+        with open(out + ".json", "w") as f:
+            json.dump(dict(meta, nparams=int(flat.size), dtype="float32",
+                           layout="W[class 0..3][row: output orbit][column: input orbit], orbit = z*16 + y*4 + x "
+                                  "in the class representative's axes"), f, indent=1)
+    return lin, meta
+
+
+def load_lin(lin, path: str = DEFAULT_LIN):
+    flat = np.fromfile(path + ".bin", dtype=np.float32)
+    lin.set_params(flat)
 
 
 def time_predict(npatch: int, reps: int, weights: str | None = DEFAULT_WEIGHTS, per_layer: bool = True):
@@ -290,16 +417,18 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
+    t.add_argument("--model", choices=("conv", "lin"), default="conv")
     t.add_argument("--npatch", type=int, default=1 << 20)
-    t.add_argument("--epochs", type=int, default=2)
+    t.add_argument("--epochs", type=int, default=None, help="default: conv 2, lin 4")
     t.add_argument("--batch", type=int, default=1024)
-    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--lr", type=float, default=None, help="default: conv 2e-3, lin 1e-3")
     t.add_argument("--seed", type=int, default=1)
-    t.add_argument("--out", default=DEFAULT_WEIGHTS)
+    t.add_argument("--out", default=None, help="default: weights/learned_init (conv), weights/lin_correction (lin)")
     t.add_argument("--eval", type=int, default=65536, help="held-out patches evaluated after training (0: none)")
     e = sub.add_parser("eval")
     e.add_argument("--npatch", type=int, default=65536)
-    e.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    e.add_argument("--weights", default=DEFAULT_WEIGHTS, help="conv net checkpoint ('' to skip)")
+    e.add_argument("--lin", default=DEFAULT_LIN, help="linear correction checkpoint ('' to skip)")
     e.add_argument("--seed", type=int, default=99)
     tm = sub.add_parser("time", help="time the network's forward pass")
     tm.add_argument("--npatch", type=int, default=65536)
@@ -309,20 +438,32 @@ def main(argv=None) -> int:
     if a.cmd == "time":
         print(json.dumps(time_predict(a.npatch, a.reps, per_layer=not a.fused_only)))
     elif a.cmd == "train":
-        net, meta = train(a.npatch, a.epochs, a.batch, a.lr, a.seed, a.out)
+        conv = a.model == "conv"
+        epochs = a.epochs if a.epochs is not None else (2 if conv else 4)
+        lr = a.lr if a.lr is not None else (2e-3 if conv else 1e-3)
+        out = a.out if a.out is not None else (DEFAULT_WEIGHTS if conv else DEFAULT_LIN)
+        fn = train if conv else train_lin
+        model, meta = fn(a.npatch, epochs, a.batch, lr, a.seed, out)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
             if a.eval:
-                print(json.dumps(evaluate(net, a.eval, 99), indent=1))
+                kw = {"net": model} if conv else {"lin": model}
+                print(json.dumps(evaluate(npatch=a.eval, seed=99, **kw), indent=1))
         import torch.distributed as dist
         if dist.is_available() and dist.is_initialized():
             dist.barrier()
             dist.destroy_process_group()
     else:
-        from gpg.net import Net
-        net = Net(max_batch=4096)
-        load(net, a.weights)
-        print(json.dumps(evaluate(net, a.npatch, a.seed), indent=1))
+        net = lin = None
+        if a.weights:
+            from gpg.net import Net
+            net = Net(max_batch=4096)
+            load(net, a.weights)
+        if a.lin:
+            from gpg.linear import LinearGuess
+            lin = LinearGuess(max_batch=1)
+            load_lin(lin, a.lin)
+        print(json.dumps(evaluate(net, lin, a.npatch, a.seed), indent=1))
     return 0
 
 

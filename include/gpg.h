@@ -59,8 +59,17 @@ enum { GPG_INIT_INTERP = 0, GPG_INIT_ZERO = 1, GPG_INIT_GUESS = 2 };
  *                  Iter+1 >= Min_Iter; cap Max_Iter (CPU_PoissonSolver_SOR.cpp:273-283)
  *   TOLERANCE:     stop once Iter+1 >= Min_Iter and the sweep's L1 residual
  *                  <= sor_tolerance * sum|Poi_Coeff*dh^2*rho|; cap Max_Iter
- *   ABS_TOLERANCE: the same with the L1 residual <= sor_tolerance */
-enum { GPG_STOP_REFERENCE = 0, GPG_STOP_TOLERANCE = 1, GPG_STOP_ABS_TOLERANCE = 2 };
+ *   ABS_TOLERANCE: the same with the L1 residual <= sor_tolerance
+ *   POT_TOLERANCE: the same with the L1 residual <= sor_tolerance * sum|phi_i|
+ *                  over the updated cells, phi_i the interpolated coarse
+ *                  potential there (taken before the initial guess replaces
+ *                  it, so every start mode gets the same bound).  The SOR
+ *                  residual stagnates at a multiple of the potential's
+ *                  rounding error, so this bound is reachable for every patch
+ *                  at any density contrast; GPG_STOP_TOLERANCE's source-scaled
+ *                  bound is not where the potential dwarfs Const*rho. */
+enum { GPG_STOP_REFERENCE = 0, GPG_STOP_TOLERANCE = 1, GPG_STOP_ABS_TOLERANCE = 2,
+       GPG_STOP_POT_TOLERANCE = 3 };
 
 /* Runtime form of the reference's compile-time shape (Makefile:13-85) plus the
  * argument list of CUAPI_Asyn_PoissonGravitySolver (Header/Prototype.h:25-34).
@@ -95,6 +104,14 @@ typedef struct gpg_params {
  * Main.cpp:1173-1223, dt = 1e-2, dh = 1, Poi_Coeff = 4*pi*1e-5, CQUAD,
  * gra_ghost = 1, Poisson and GraAcc on. */
 GPG_API int gpg_default_params(gpg_params *p, int real_size, int ghost, int scheme);
+
+/* The calibrated fixed residual for GPG_STOP_POT_TOLERANCE at (real_size,
+ * ghost): 2 x the 90th percentile of L1 residual / sum|interpolated phi| at
+ * the reference's own stopping point (CPU_PoissonSolver_SOR.cpp:275-281) of
+ * zero-start SOR on seeded power-law inputs -- the round-off floor the
+ * reference rule stops at, reachable by every patch.  FP32: 9.8e-7 (ghost 1)
+ * ... 1.4e-6 (ghost 5); FP64: 1.8e-15 ... 2.5e-15.  No reference counterpart. */
+GPG_API int gpg_pot_tolerance(int real_size, int ghost, double *tol);
 
 /* Check a parameter block (same checks as CUAPI_Asyn_PoissonGravitySolver.cu:116-140). */
 GPG_API int gpg_validate_params(const gpg_params *p);
@@ -295,6 +312,64 @@ GPG_API int gpg_net_apply_gradient(gpg_net *net, const float *d_grad, float lr, 
 /* GPG_ERR_CUDA when a tensor-core wait timed out in an earlier call */
 GPG_API int gpg_net_check(gpg_net *net);
 GPG_API const char *gpg_net_last_error(void);
+
+/* ---------------------------------------------------------------------------
+ * Learned linear correction of the interpolated start, fused into ghost-size-1
+ * FP32 SOR.  No reference counterpart (the reference starts from the
+ * interpolated coarse potential, CPU_PoissonSolver_SOR.cpp:80-209, and runs
+ * SOR from there).  The start value is phi_i + delta: phi_i the interpolated
+ * coarse potential, delta a learned linear function of the residual
+ * r0 = Lap(phi_i) - Const*rho of that start on the 8^3 interior.  The map is
+ * equivariant under the reflections of the cube: r0 is folded by a length-8
+ * Walsh-Hadamard transform per mirror orbit into 8 parity blocks of 64, block
+ * b is multiplied by the 64 x 64 matrix of its class (number of odd axes,
+ * 0..3; blocks of one class share it through an axis permutation of the orbit
+ * index) and the result unfolded.  Parameters: W[4][64][64] FP32, row =
+ * output orbit, column = input orbit, orbit o = k*16 + j*4 + i (z, y, x in
+ * [0,4), the class representative's axes).  The solve runs the fold, the BF16
+ * tcgen05 MMAs (FP32 accumulation), the unfold and the SOR sweeps in one
+ * persistent kernel; the correction never leaves the chip.
+ * ------------------------------------------------------------------------- */
+typedef struct gpg_lin gpg_lin;
+/* max_batch bounds npatch of gpg_lin_gradients / gpg_lin_train_step only;
+ * parameters start at zero (delta = 0: the plain interpolated start) */
+GPG_API int gpg_lin_create(gpg_lin **lin, int max_batch, int device_id);
+GPG_API int gpg_lin_destroy(gpg_lin *lin);
+GPG_API int gpg_lin_param_count(int64_t *count);
+GPG_API int gpg_lin_get_params(gpg_lin *lin, float *host_params);
+GPG_API int gpg_lin_set_params(gpg_lin *lin, const float *host_params);
+/* Stream-ordered solve with the learned start: the arguments and outputs of
+ * gpg_poisson_gravity_device for p->ghost == 1, p->real_size == 4, SOR (any
+ * stopping rule, output window and fused gravity update; p->init_mode is
+ * ignored).  d_pot_out [P][GRA_NXT]^3, d_flu [P][5][8]^3 when p->gra_acc. */
+GPG_API int gpg_lin_solve_device(gpg_lin *lin, const gpg_params *p, int npatch, const float *d_rho,
+                                 const float *d_pot_in, float *d_pot_out, float *d_flu, int32_t *d_iters,
+                                 double *d_resid, void *stream);
+/* Training features (stream-ordered): d_u [P][8][64] the folded residual of
+ * each patch (block b at b*64, orbit index in its class's axes); when
+ * d_target [P][8]^3 (a converged interior potential) is given, d_t [P][8][64]
+ * the folded (target - interpolated start) / 8, so that the unfold of
+ * W u ~ t is the correction. */
+GPG_API int gpg_lin_features(gpg_lin *lin, const gpg_params *p, int npatch, const float *d_rho,
+                             const float *d_pot_in, const float *d_target, float *d_u, float *d_t, void *stream);
+/* loss = mean over patches, blocks and rows of (s_p (W u - t))^2, s_p the
+ * power of two with max|u_p| s_p in [0.5, 1); its gradient wrt W into d_grad
+ * [16384] (may be NULL: kept inside) and the loss into d_loss (may be NULL) */
+GPG_API int gpg_lin_gradients(gpg_lin *lin, int npatch, const float *d_u, const float *d_t, float *d_grad,
+                              float *d_loss, void *stream);
+/* gradients + one Adam step (beta 0.9 / 0.999, eps 1e-8) */
+GPG_API int gpg_lin_train_step(gpg_lin *lin, int npatch, const float *d_u, const float *d_t, float lr,
+                               float *d_loss, void *stream);
+/* one Adam step with a caller-supplied gradient (data-parallel training) */
+GPG_API int gpg_lin_apply_gradient(gpg_lin *lin, const float *d_grad, float lr, void *stream);
+/* GPG_ERR_CUDA when a tensor-core wait of an earlier solve timed out; reading
+ * the flag clears it */
+GPG_API int gpg_lin_check(gpg_lin *lin);
+/* Test hook: with polls > 0 every later solve also makes one bounded wait of
+ * that many polls on a barrier nothing signals, so the timeout path runs
+ * (the solve itself completes normally); 0 switches it off. */
+GPG_API int gpg_lin_set_wait_probe(gpg_lin *lin, int polls);
+GPG_API const char *gpg_lin_last_error(void);
 
 #ifdef __cplusplus
 }

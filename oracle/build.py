@@ -27,7 +27,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# the reference tree: $GPG_REFERENCE_ROOT, else a checkout named "reference"
+# beside this repository; absent trees are skipped by build_ref/build_integration
+DEFAULT_REF = os.environ.get("GPG_REFERENCE_ROOT") or os.path.join(os.path.dirname(REPO), "reference")
 
 REF_SOURCES = [
     "CPU_Solver/CPU_PoissonGravitySolver.cpp",

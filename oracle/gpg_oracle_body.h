@@ -369,6 +369,12 @@ int FN(oracle_poisson_gravity)(const gpg_params *prm, int npatch, const T *rho_a
          for (int P = 0; P < npatch; P++) {
             const T *rho = rho_all + (size_t)P * sr;
             FN(oracle_interp)(pin_all + (size_t)P * sp, cube, g, prm->int_scheme);
+            double pot_sum = 0.0;   /* GPG_STOP_POT_TOLERANCE scale, before the guess */
+            if (prm->stop_mode == GPG_STOP_POT_TOLERANCE)
+               for (int c = 0; c < M; c++)
+               for (int b = 0; b < M; b++)
+               for (int a = 0; a < M; a++)
+                  pot_sum += (double)TABS(cube[((size_t)(c + 1) * N + (b + 1)) * N + (a + 1)]);
             if (prm->init_mode != GPG_INIT_INTERP)
                for (int c = 0; c < M; c++)
                for (int b = 0; b < M; b++)
@@ -381,6 +387,8 @@ int FN(oracle_poisson_gravity)(const gpg_params *prm, int npatch, const T *rho_a
                double s = 0.0;
                for (size_t t = 0; t < sr; t++) s += (double)TABS(Const * rho[t]);
                tol_abs = prm->sor_tolerance * s;
+            } else if (prm->stop_mode == GPG_STOP_POT_TOLERANCE) {
+               tol_abs = prm->sor_tolerance * pot_sum;
             }
             double r = 0.0;
             const int it = FN(oracle_sor_patch)(cube, rho, g, Const, Omega_6, prm->sor_min_iter,

@@ -50,7 +50,7 @@ def test_c_defaults_equal_python_defaults(rs, g, scheme):
 
 @pytest.mark.parametrize("field,value", [("ghost", 0), ("ghost", 6), ("gra_ghost", 3), ("int_scheme", 1),
                                          ("real_size", 2), ("scheme", 3), ("init_mode", 7),
-                                         ("stop_mode", 3), ("sor_max_iter", -1), ("p5_gradient", 1)])
+                                         ("stop_mode", 4), ("sor_max_iter", -1), ("p5_gradient", 1)])
 def test_validation_rejects(field, value):
     p = default_params(4, 1, GPG_SOR).copy(**{field: value})
     rc = library().gpg_validate_params(C.byref(p))

@@ -131,17 +131,19 @@ def test_fused_predict_matches_layers(torch, npatch):
 def test_learned_guess_reduces_sweeps(torch):
     """A network trained briefly on the plain SOR's own solutions (ghost 1,
     rho0 log-uniform, power index in [1.5, 2.5]) starts the SOR closer to the
-    solution: fewer sweeps to the same relative L1 tolerance on held-out
-    patches, at the same error against the FP64 solution."""
+    solution: fewer sweeps to the calibrated fixed residual on held-out
+    patches, at the same error against the FP64 solution.  (Its inference
+    costs far more than the sweeps it saves: the throughput comparison is
+    recorded by learned.evaluate and asserted for the linear correction.)"""
     import learned
     net, meta = learned.train(npatch=65536, epochs=2, batch=512, lr=2e-3, seed=3, out=None, log=lambda *a: None)
     assert meta["loss_history"][-1][1] < 0.1 * meta["loss_history"][0][1] or meta["loss_history"][-1][1] < 1e-3
-    r = learned.evaluate(net, 4096, seed=77)
-    plain, guess = r["plain_zero_start"], r["learned_init"]
+    r = learned.evaluate(net=net, npatch=4096, seed=77, reps=1, rule=False)
+    plain, guess = r["plain_zero_start"], r["learned_conv"]
     assert guess["sweeps"]["mean"] < 0.85 * plain["sweeps"]["mean"], r
     assert guess["sweeps"]["p50"] < plain["sweeps"]["p50"], r
-    # both stop at the same residual tolerance: same error scale against FP64
-    assert guess["rel_linf_vs_fp64"] <= 3 * plain["rel_linf_vs_fp64"] + 1e-6, r
+    # both stop at the same fixed residual: same error scale against FP64
+    assert guess["rel_linf_vs_fp64"]["max"] <= 3 * plain["rel_linf_vs_fp64"]["max"] + 1e-6, r
     net.close()
 
 

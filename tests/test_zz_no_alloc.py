@@ -13,7 +13,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from gpg.abi import GPG_INIT_ZERO, GPG_SOR, GPG_STOP_ABS_TOLERANCE, GpgBatchGroup, GpgParams, default_params
+from gpg.abi import (GPG_ERR_INVALID, GPG_INIT_ZERO, GPG_OK, GPG_SOR, GPG_STOP_ABS_TOLERANCE, GpgBatchGroup,
+                     GpgParams, default_params)
 from gpg.inputs import log_uniform, make_patches, mixed_ghost_assignment
 
 pytestmark = pytest.mark.gpu
@@ -114,5 +115,49 @@ def test_noalloc_rejects_batches_beyond_its_limit():
     arr[0].npatch = (1 << 30) + 1  # more than one call may queue; rejected on the host, nothing launched
     p = default_params(4, 1, GPG_SOR)
     rc = noalloc(C.byref(p), 1, arr, C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
-    assert rc == 1
+    assert rc == GPG_ERR_INVALID
     assert b"exceeds" in lib.gpg_last_error()
+
+
+def test_noalloc_empty_batches_launch_nothing():
+    """No groups, or groups without patches: the call succeeds, writes no
+    output and a following full call still matches the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gpg.lib import library
+    lib = library()
+    noalloc = lib.gpg_solve_batch_device_noalloc
+    noalloc.restype = C.c_int
+    noalloc.argtypes = [C.POINTER(GpgParams), C.c_int, C.POINTER(GpgBatchGroup), C.c_void_p]
+    dev = torch.device("cuda:0")
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    p = default_params(4, 1, GPG_SOR, init_mode=GPG_INIT_ZERO, stop_mode=GPG_STOP_ABS_TOLERANCE,
+                       sor_tolerance=1e-4, sor_min_iter=1, sor_max_iter=200)
+    assert noalloc(C.byref(p), 0, None, stream) == GPG_OK, lib.gpg_last_error()
+    groups = _groups(torch, 4, 60, seed=9, dev=dev)
+    arr = _c_groups(groups)
+    for a in arr:
+        a.npatch = 0
+    for g in groups:
+        g["iters"].fill_(-7)
+    assert noalloc(C.byref(p), len(groups), arr, stream) == GPG_OK, lib.gpg_last_error()
+    torch.cuda.synchronize()
+    assert all(bool((g["iters"] == -7).all()) for g in groups)
+    arr = _c_groups(groups)
+    for g in groups:
+        g["flu"].copy_(g["flu0"])
+    assert noalloc(C.byref(p), len(groups), arr, stream) == GPG_OK, lib.gpg_last_error()
+    torch.cuda.synchronize()
+    got = _snapshot(groups)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    for g in groups:
+        g["flu"].copy_(g["flu0"])
+    alloc = lib.gpg_solve_batch_device
+    alloc.restype = C.c_int
+    alloc.argtypes = [C.POINTER(GpgParams), C.c_int, C.POINTER(GpgBatchGroup), C.c_void_p, C.c_void_p]
+    assert alloc(C.byref(p), len(groups), arr, C.c_void_p(counter.data_ptr()), stream) == GPG_OK
+    torch.cuda.synchronize()
+    for (gp, gf, gi, gr), g in zip(got, groups):
+        assert torch.equal(g["pot_out"], gp) and torch.equal(g["flu"], gf)
+        assert torch.equal(g["iters"], gi) and torch.equal(g["resid"], gr)
