@@ -101,12 +101,16 @@ int ensure_smem(KernelFn *fn, size_t bytes, AttrOnce &st, int *max_threads = nul
 // SOR kernel variants: (teams per CTA, phased pass).  The table below holds
 // the variant per (precision, ghost size); defaults are the fastest measured
 // on B200, gpg_set_sor_variant / a tuning file override them.
-constexpr int kSorVariants = 14;
-constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4, 1, 1, 2, 2, 1, 1, 1, 1};
-constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true, false,
-                                                  true,  false, true, false, true, false, true};
-constexpr int kSorVariantSplit[kSorVariants] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 1, 1};  // lanes per column
-constexpr int kSorVariantRows[kSorVariants] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2};   // rows per lane
+// Variants 14-16: the layouts of 10, 11 and 13 in the staged persistent
+// kernel (patches per CTA reported as 0: teams per CTA chosen per shape).
+constexpr int kSorVariants = 17;
+constexpr int kSorVariantPPC[kSorVariants] = {1, 1, 2, 2, 4, 4, 1, 1, 2, 2, 1, 1, 1, 1, 0, 0, 0};
+constexpr bool kSorVariantPhased[kSorVariants] = {false, true, false, true, false, true, false, true,  false,
+                                                  true,  false, true, false, true, false, true, true};
+constexpr int kSorVariantSplit[kSorVariants] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 1, 1, 2, 2, 1};  // lanes per column
+constexpr int kSorVariantRows[kSorVariants] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2};   // rows per lane
+constexpr bool kSorVariantStaged[kSorVariants] = {false, false, false, false, false, false, false, false, false,
+                                                  false, false, false, false, false, true,  true,  true};
 // atomic: gpg_set_sor_variant may run on one host thread while another launches
 std::atomic<int> g_sor_variant[2][6] = {
     // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
@@ -184,6 +188,60 @@ int prepare_sor_v() {
   }
 }
 
+// Staged persistent kernel: CTAs of about 128 threads, as many as fit on the
+// device (per-device occupancy), at most one team per patch.  Inputs that are
+// not 16-byte aligned (bulk copies need it) run the same layout unstaged.
+template <typename T, int G, bool PHASED, int Z, int Y>
+int launch_staged_v(const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  if constexpr (!gpg::SorCfg<T, G, Z, Y>::FITS) {
+    return fail(GPG_ERR_UNSUPPORTED, "SOR variant holds more state per lane than registers allow");
+  } else {
+    constexpr int TEAM = gpg::SorCfg<T, G, Z, Y>::TEAM;
+    constexpr int TPC = TEAM >= 128 ? 1 : 128 / TEAM;
+    using SS = gpg::StagedSmem<T, G, Z, Y, TPC>;
+    if ((reinterpret_cast<uintptr_t>(a.rho) | reinterpret_cast<uintptr_t>(a.pot_in)) & 15)
+      return launch_sor_v<T, G, 1, PHASED, Z, Y>(a, s);
+    if (SS::bytes > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "staged SOR needs %zu bytes of shared memory", SS::bytes);
+    auto fn = gpg::staged_sor_kernel<T, G, PHASED, Z, Y, TPC>;
+    static AttrOnce attr;
+    int max_threads = 0;
+    if (int rc = ensure_smem(fn, SS::bytes, attr, &max_threads)) return rc;
+    if (TPC * TEAM > max_threads)
+      return fail(GPG_ERR_UNSUPPORTED, "staged SOR needs %d threads per CTA (registers allow %d)", TPC * TEAM,
+                  max_threads);
+    static int resident[kMaxDevices] = {};  // CTAs per device
+    int dev = 0;
+    if (int rc = current_device(&dev)) return rc;
+    if (!resident[dev]) {
+      int sms = 0, per = 0;
+      GPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      GPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, TPC * TEAM, SS::bytes));
+      if (per < 1) return fail(GPG_ERR_UNSUPPORTED, "staged SOR does not fit on an SM");
+      resident[dev] = sms * per;
+    }
+    const int64_t need = (a.npatch + TPC - 1) / TPC;
+    const int64_t grid = std::min<int64_t>(need, resident[dev]);
+    fn<<<(unsigned)grid, TPC * TEAM, SS::bytes, s>>>(a);
+    GPG_CUDA(cudaGetLastError());
+    return GPG_OK;
+  }
+}
+
+template <typename T, int G, bool PHASED, int Z, int Y>
+int prepare_staged_v() {
+  if constexpr (!gpg::SorCfg<T, G, Z, Y>::FITS) {
+    return fail(GPG_ERR_UNSUPPORTED, "SOR variant holds more state per lane than registers allow");
+  } else {
+    constexpr int TEAM = gpg::SorCfg<T, G, Z, Y>::TEAM;
+    constexpr int TPC = TEAM >= 128 ? 1 : 128 / TEAM;
+    using SS = gpg::StagedSmem<T, G, Z, Y, TPC>;
+    if (SS::bytes > 227 * 1024) return fail(GPG_ERR_UNSUPPORTED, "staged SOR needs %zu bytes of shared memory", SS::bytes);
+    static AttrOnce attr;
+    if (int rc = ensure_smem(gpg::staged_sor_kernel<T, G, PHASED, Z, Y, TPC>, SS::bytes, attr)) return rc;
+    return prepare_sor_v<T, G, 1, PHASED, Z, Y>();  // the unstaged fallback
+  }
+}
+
 template <typename T, int G>
 int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   std::call_once(g_tune_once, load_tune_file);
@@ -201,7 +259,10 @@ int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
     case 10: return launch_sor_v<T, G, 1, false, 2, 2>(a, s);
     case 11: return launch_sor_v<T, G, 1, true, 2, 2>(a, s);
     case 12: return launch_sor_v<T, G, 1, false, 1, 2>(a, s);
-    default: return launch_sor_v<T, G, 1, true, 1, 2>(a, s);
+    case 13: return launch_sor_v<T, G, 1, true, 1, 2>(a, s);
+    case 14: return launch_staged_v<T, G, false, 2, 2>(a, s);
+    case 15: return launch_staged_v<T, G, true, 2, 2>(a, s);
+    default: return launch_staged_v<T, G, true, 1, 2>(a, s);
   }
 }
 
@@ -222,7 +283,10 @@ int prepare_sor() {
     case 10: return prepare_sor_v<T, G, 1, false, 2, 2>();
     case 11: return prepare_sor_v<T, G, 1, true, 2, 2>();
     case 12: return prepare_sor_v<T, G, 1, false, 1, 2>();
-    default: return prepare_sor_v<T, G, 1, true, 1, 2>();
+    case 13: return prepare_sor_v<T, G, 1, true, 1, 2>();
+    case 14: return prepare_staged_v<T, G, false, 2, 2>();
+    case 15: return prepare_staged_v<T, G, true, 2, 2>();
+    default: return prepare_staged_v<T, G, true, 1, 2>();
   }
 }
 
@@ -680,6 +744,12 @@ extern "C" int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phas
   if (variant < 0 || variant >= kSorVariants) return fail(GPG_ERR_INVALID, "variant %d", variant);
   if (patches_per_cta) *patches_per_cta = kSorVariantPPC[variant];
   if (phased) *phased = kSorVariantPhased[variant];
+  return GPG_OK;
+}
+
+extern "C" int gpg_sor_variant_staged(int variant, int *staged) {
+  if (variant < 0 || variant >= kSorVariants) return fail(GPG_ERR_INVALID, "variant %d", variant);
+  if (staged) *staged = kSorVariantStaged[variant];
   return GPG_OK;
 }
 

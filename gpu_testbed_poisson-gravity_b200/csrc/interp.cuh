@@ -12,9 +12,10 @@
 
 namespace gpg {
 
-// `coarse` is one patch's [POT_NXT]^3 potential (global memory, read through
-// L1: each value feeds up to 27 coarse cells).
-template <typename T, int G, int NT, typename Store>
+// `coarse` is one patch's [POT_NXT]^3 potential: in global memory, read
+// through L1 (LDG; each value feeds up to 27 coarse cells), or a copy staged
+// in shared memory (!LDG).
+template <typename T, int G, int NT, bool LDG = true, typename Store>
 __device__ __forceinline__ void interpolate(const T *__restrict__ coarse, int tid, int int_scheme,
                                             Store store) {
   using g = Geo<G>;
@@ -22,7 +23,11 @@ __device__ __forceinline__ void interpolate(const T *__restrict__ coarse, int ti
   for (int w = tid; w < NC * NC * NC; w += NT) {
     const int i = 1 + w % NC, j = 1 + (w / NC) % NC, k = 1 + w / (NC * NC);
     const T *c0 = coarse + (k * PN + j) * PN + i;
-    auto C = [c0](int dk, int dj, int di) -> T { return __ldg(c0 + (dk * PN + dj) * PN + di); };
+    auto C = [c0](int dk, int dj, int di) -> T {
+      const T *q = c0 + (dk * PN + dj) * PN + di;
+      if constexpr (LDG) return __ldg(q);
+      else return *q;
+    };
     T child[8];
     if (int_scheme == 4) {
       const T c8 = T(0.125), c64 = T(0.015625), c512 = T(0.001953125);

@@ -19,16 +19,22 @@
 // 4 x 64 x 64 parameters (FP32 masters, BF16 in the kernel), 65,536 FLOP per
 // patch (algorithmic).
 //
-// Kernel.  CTA = 8 warps; each warp is one SOR team (the two-row, split-column
-// lane layout of sor_kernel.cuh) and owns one patch of the CTA's batch of 8.
-// Per batch, every team interpolates its patch into its shared cube, forms r0
-// for its cells, folds it and writes the 8 block vectors (BF16) into the MMA
-// operand tile; thread 0 issues 16 tcgen05.mma (M 128 = two class matrices
-// stacked, N 16 = the 8 patches of two blocks side by side, K 64) against the
-// weight tiles, which stay in shared memory for the whole kernel; the teams
-// read the FP32 results back from TMEM, unfold their own patch, add the
-// correction to the cube and run the ordinary sweeps, stopping rule, output
-// window and (optionally) gravity update of sor_solve_patch_with.
+// Kernel.  One persistent CTA per SM, 16 warps in two independent halves of
+// 8 that share the weight tiles (each half has its own barrier, operand tile,
+// TMEM columns and MMA barrier, so one half's batch synchronisation is hidden
+// behind the other's work).  Each warp is one SOR team (the two-row,
+// split-column lane layout of sor_kernel.cuh) and owns one patch of its
+// half's batch of 8.  A warp's next patch (coarse potential and density,
+// 4 KB) is prefetched into shared memory with bulk copies while the current
+// one is solved.  Per batch, every team interpolates its patch from the
+// staged copy into its shared cube, forms r0 for its cells, folds it and
+// writes the 8 block vectors (BF16) into its half's MMA operand tile; one
+// thread per half issues 16 tcgen05.mma (M 128 = two class matrices stacked,
+// N 16 = the 8 patches of two blocks side by side, K 64) against the weight
+// tiles, which stay in shared memory for the whole kernel; the teams read the
+// FP32 results back from TMEM, unfold their own patch, add the correction to
+// the cube and run the ordinary sweeps, stopping rule, output window and
+// (optionally) gravity update of sor_solve_patch_with.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -39,15 +45,23 @@
 namespace gpg {
 namespace lin {
 
-constexpr int kWarps = 8;             // teams (patches) per CTA batch
-constexpr int kThreads = kWarps * 32;
-constexpr int kN = 2 * kWarps;        // MMA N: two blocks' patches side by side
+constexpr int kHalfWarps = 8;         // teams (patches) per batch of one group of teams
+constexpr int kN = 2 * kHalfWarps;    // MMA N: two blocks' patches side by side
 constexpr int kGroups = 4;            // MMAs per K step: (c0 | c3), 3 x (c1 | c2)
 constexpr int kK = 64;                // orbits per block
 constexpr int kTileBytes = 128 * kK * 2;       // one A tile (BF16): 16 KB
-constexpr int kGroupBytes = kN * kK * 2;       // one B tile (BF16): 2 KB
-constexpr int kTmemCols = kGroups * kN;        // 64
+// one B tile (BF16): 8 K chunks of kN rows x 16 B, chunks kChunkB apart (16 B
+// of padding put consecutive chunks on different banks for the operand stores)
+constexpr int kChunkB = kN * 16 + 16;
+constexpr int kGroupBytes = (kK / 8) * kChunkB;
+// team scratch: interior cell (z, y, x) at z * kScrPZ + y * 8 + x (plane pitch
+// padded from 64 so that lane-cell and mirror-orbit accesses spread over the
+// banks), block results at b * 64 + o
+constexpr int kScrPZ = 66;
+constexpr int kScrWords = 8 * kScrPZ;
+constexpr int kHalfCols = kGroups * kN;        // TMEM columns of one group of teams: 64
 constexpr int kParams = 4 * kK * kK;           // 16,384
+constexpr int kFeatureGain = 17;               // log2 of the training features' extra scale
 constexpr uint32_t kIdesc = tc::idesc_bf16(128, kN, false, false);
 
 // block b = pz*4 + py*2 + px: MMA group, side (rows 0-63 / 64-127 of the
@@ -67,11 +81,13 @@ __host__ __device__ constexpr int perm_orbit(int o, int t) {
   const int k = o >> 4, j = (o >> 2) & 3, i = o & 3;
   return t == 0 ? o : (t == 1 ? (k << 4) | (i << 2) | j : (t == 2 ? (i << 4) | (j << 2) | k : (j << 4) | (k << 2) | i));
 }
-// interior index (z*8 + y)*8 + x of orbit o's image under mirror s = (sz, sy, sx)
+// scratch word of interior cell (z, y, x)
+__host__ __device__ constexpr int scr_cell(int z, int y, int x) { return z * kScrPZ + y * 8 + x; }
+// scratch word of orbit o's image under mirror s = (sz, sy, sx)
 __host__ __device__ constexpr int orbit_cell(int o, int s) {
   const int k = o >> 4, j = (o >> 2) & 3, i = o & 3;
   const int z = (s & 4) ? 7 - k : k, y = (s & 2) ? 7 - j : j, x = (s & 1) ? 7 - i : i;
-  return (z * 8 + y) * 8 + x;
+  return scr_cell(z, y, x);
 }
 
 // In-place length-8 Walsh-Hadamard transform, stages x, y, z (index bit 0, 1,
@@ -99,7 +115,22 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void cta_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+// named barrier of one group of teams (ids 1.., 0 is __syncthreads)
+__device__ __forceinline__ void half_bar(int half) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + half), "n"(kHalfWarps * 32) : "memory");
+}
+
+// Launch shape: HALVES groups of 8 teams share the weight tiles; STAGE: each
+// team prefetches its next patch's inputs into shared memory (bulk copies).
+// Shared memory allows 2 staged groups or 3 unstaged ones (registers then
+// bounded to 80 per thread).
+template <int HALVES, bool STAGE>
+struct Shape {
+  static constexpr int kHalves = HALVES;
+  static constexpr int kWarps = HALVES * kHalfWarps;
+  static constexpr int kThreads = kWarps * 32;
+  static constexpr int kTmemCols = HALVES * kHalfCols <= 128 ? 128 : 256;  // a power of two
+};
 
 // Team shape: ghost 1, FP32, two rows per lane, split column (variant 10 of
 // the per-ghost-size kernels): one warp per patch, every lane owns cells.
@@ -107,20 +138,27 @@ using Cfg = SorCfg<float, 1, 2, 2>;
 using Smem = SorSmem<float, 1, 2, 2>;
 static_assert(Cfg::TEAM == 32 && Cfg::NBLOCK * Cfg::BLOCK == 32, "one fully used warp per patch");
 
+template <int HALVES, bool STAGE>
 struct Layout {
-  static constexpr size_t a_off = 0;                                   // 2 weight tiles
-  static constexpr size_t b_off = a_off + 2 * kTileBytes;              // 4 operand tiles
-  static constexpr size_t scr_off = b_off + kGroups * kGroupBytes;     // per team 512 floats
-  static constexpr size_t cube_off = scr_off + kWarps * 512 * 4;       // per team cube
-  static constexpr size_t bar_off = cube_off + kWarps * Smem::team_bytes;
-  static constexpr size_t bytes = bar_off + 64;
+  using SH = Shape<HALVES, STAGE>;
+  static constexpr int kStage = Geo<1>::PN3 + Geo<1>::RHO3;               // floats per staged patch
+  static constexpr size_t a_off = 0;                                      // 2 weight tiles
+  static constexpr size_t b_off = a_off + 2 * kTileBytes;                 // per group 4 operand tiles
+  static constexpr size_t scr_off = b_off + HALVES * kGroups * kGroupBytes;  // per team scratch
+  static constexpr size_t stg_off = scr_off + SH::kWarps * kScrWords * 4;    // per team staged inputs
+  static constexpr size_t cube_off = stg_off + (STAGE ? SH::kWarps * kStage * 4 : 0);  // per team cube
+  static constexpr size_t bar_off = cube_off + SH::kWarps * Smem::team_bytes;
+  // barriers: [0, HALVES) MMA done per group, then staged inputs per team, then the probe
+  static constexpr int kBars = HALVES + SH::kWarps + 1;
+  static constexpr size_t bytes = bar_off + kBars * 8 + 16;
+  static_assert(bytes <= 227 * 1024, "shared memory");
 };
 
 struct LinArgs {
   SolveArgs<float> s;
   const __nv_bfloat16 *wtiles;  // [2][kTileBytes / 2], packed by the host
-  float *u_out;                 // features mode: [P][8][64] folded residual (class axes)
-  float *t_out;                 // features mode: [P][8][64] folded (target - interpolation) / 8
+  float *u_out;                 // features mode: [P][8][64] folded residual (class axes), scaled
+  float *t_out;                 // features mode: [P][8][64] folded (target - interpolation) / 8, scaled
   const float *target;          // features mode: [P][8]^3 or null
   int *err;                     // set when a tensor-core wait timed out
   int probe_polls;              // > 0: thread 0 also waits that many polls on a barrier nothing signals
@@ -163,24 +201,39 @@ __device__ __forceinline__ void lane_residual(const SorLaneState<float, 1, 2, 2>
   }
 }
 
-// interior index of the lane's colour-p cell at local height z in row r
-__device__ __forceinline__ int lane_cell(const SorLaneState<float, 1, 2, 2> &st, int r, int p, int z) {
+// interior (z, y, x) of the lane's colour-p cell at local height z in row r
+__device__ __forceinline__ void lane_xyz(const SorLaneState<float, 1, 2, 2> &st, int r, int p, int z, int &cz,
+                                         int &cy, int &cx) {
   const int yr = st.y + r, zg = st.zbase + z;
-  const int x = ((yr + zg + p) & 1) == 0 ? 2 * st.h + 1 : 2 * st.h + 2;
-  return ((zg - 1) * 8 + (yr - 1)) * 8 + (x - 1);
+  cx = (((yr + zg + p) & 1) == 0 ? 2 * st.h + 1 : 2 * st.h + 2) - 1;
+  cy = yr - 1;
+  cz = zg - 1;
+}
+// its scratch word
+__device__ __forceinline__ int lane_cell(const SorLaneState<float, 1, 2, 2> &st, int r, int p, int z) {
+  int cz, cy, cx;
+  lane_xyz(st, r, p, z, cz, cy, cx);
+  return scr_cell(cz, cy, cx);
 }
 
-template <bool FEATURES>
-__global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
+template <bool FEATURES, int HALVES, bool STAGE>
+__global__ void __launch_bounds__(Shape<HALVES, STAGE>::kThreads, 1) lin_sor_kernel(const LinArgs a) {
+  using SH = Shape<HALVES, STAGE>;
+  using Layout = gpg::lin::Layout<HALVES, STAGE>;
+  constexpr int kHalves = SH::kHalves, kWarps = SH::kWarps, kThreads = SH::kThreads, kTmemCols = SH::kTmemCols;
+  constexpr bool kStaged = STAGE && !FEATURES;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *sA = smem + Layout::a_off;
-  unsigned char *sB = smem + Layout::b_off;
   float *s_scr = reinterpret_cast<float *>(smem + Layout::scr_off);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + Layout::bar_off);  // [0] MMA done, [1] probe
-  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 2);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + Layout::bar_off);
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + Layout::kBars);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float *scr = s_scr + warp * 512;
+  const int half = warp / kHalfWarps, wl = warp - half * kHalfWarps;  // team index inside the half
+  unsigned char *sB = smem + Layout::b_off + size_t(half) * kGroups * kGroupBytes;
+  float *scr = s_scr + warp * kScrWords;
+  float *stg = reinterpret_cast<float *>(smem + Layout::stg_off) + size_t(warp) * Layout::kStage;
   unsigned char *tb = smem + Layout::cube_off + size_t(warp) * Smem::team_bytes;
+  uint64_t *bar_mma = bars + half, *bar_stg = bars + kHalves + warp, *bar_probe = bars + kHalves + kWarps;
 
   uint32_t tmem = 0;
   if constexpr (!FEATURES) {
@@ -189,8 +242,7 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
     uint4 *dst = reinterpret_cast<uint4 *>(sA);
     for (int i = tid; i < 2 * kTileBytes / 16; i += kThreads) dst[i] = src[i];
     if (tid == 0) {
-      tc::mbar_init(&bars[0], 1);
-      tc::mbar_init(&bars[1], 1);
+      for (int i = 0; i < Layout::kBars; ++i) tc::mbar_init(&bars[i], 1);
       tc::mbar_fence_init();
     }
     if (warp == 0) {
@@ -201,24 +253,50 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    tmem = *s_tmem;
+    tmem = *s_tmem + uint32_t(half * kHalfCols);
     if (a.probe_polls > 0 && tid == 0) {
       // test hook: a bounded wait on a barrier nothing arrives on gives up
       // after probe_polls polls, records the timeout and the kernel goes on
-      tc::mbar_wait_polls(&bars[1], 0, a.err, uint32_t(a.probe_polls));
+      tc::mbar_wait_polls(bar_probe, 0, a.err, uint32_t(a.probe_polls));
     }
   }
   const int64_t npatch = a.s.npatch;
-  const int64_t nbatch = (npatch + kWarps - 1) / kWarps;
-  uint32_t phase = 0, last_parity = 0;
-  bool late = false;  // a wait for the MMAs gave up
-  for (int64_t batch = blockIdx.x; batch < nbatch; batch += gridDim.x) {
-    const int64_t mine = batch * kWarps + warp;
+  const int64_t nbatch = (npatch + kHalfWarps - 1) / kHalfWarps;
+  const int64_t hstride = int64_t(gridDim.x) * kHalves;
+  // the patch team wl solves in batch b; a team past the end solves the last
+  // patch again without storing it, so that it takes part in the barriers
+  auto patch_of = [&](int64_t b) {
+    const int64_t m = b * kHalfWarps + wl;
+    return m < npatch ? m : npatch - 1;
+  };
+  auto stage = [&](int64_t P) {  // lane 0: this team's inputs of patch P -> stg
+    tc::mbar_arrive_expect_tx(bar_stg, uint32_t(Layout::kStage * 4));
+    tc::bulk_load(stg, a.s.pot_in + P * Geo<1>::PN3, Geo<1>::PN3 * 4, bar_stg);
+    tc::bulk_load(stg + Geo<1>::PN3, a.s.rho + P * Geo<1>::RHO3, Geo<1>::RHO3 * 4, bar_stg);
+  };
+  const int64_t first = int64_t(blockIdx.x) * kHalves + half;
+  if constexpr (kStaged) {
+    if (first < nbatch && lane == 0) stage(patch_of(first));
+  }
+  uint32_t it = 0, phase = 0, last_parity = 0;
+  bool late = false;  // a bounded wait gave up
+  for (int64_t batch = first; batch < nbatch; batch += hstride, ++it) {
+    const int64_t mine = batch * kHalfWarps + wl;
     const bool real = mine < npatch;
-    // a team past the end solves the last patch again without storing it, so
-    // that every team takes part in the batch's barriers
-    const int64_t P_ = real ? mine : npatch - 1;
+    const int64_t P_ = patch_of(batch), next = batch + hstride;
+    if constexpr (kStaged) {
+      if (!tc::mbar_wait(bar_stg, it & 1u, a.err)) late = true;
+    }
     auto hook = [&](const auto &st) {
+      if constexpr (kStaged) {
+        // the staged inputs are in the cube and registers: prefetch the
+        // team's next patch while this one is corrected and solved
+        __syncwarp();
+        if (next < nbatch && lane == 0) {
+          tc::fence_proxy_async_smem();
+          stage(patch_of(next));
+        }
+      }
       float res[2][2][Cfg::MH];
       lane_residual(st, res);
 #pragma unroll
@@ -238,12 +316,29 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
         hadamard8(u[oo]);
       }
       if constexpr (FEATURES) {
+        // scale: 2^(kFeatureGain - e) with max|phi_i| over the interior =
+        // m 2^e, m in [0.5, 1) -- exact, and a linear map is indifferent to
+        // it; the training loss then weights patches by their potential, and
+        // the gain puts the residuals (about 1e-5 of the potential) near one,
+        // far above the optimizer's epsilon
+        float vmax = 0.f;
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int z = 1; z <= Cfg::MH; ++z) vmax = fmaxf(vmax, fabsf(st.v[r][p][z]));
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, m));
+        int ex = 0;
+        frexpf(vmax, &ex);
+        const float sc = ldexpf(1.f, (vmax > 0.f ? -ex : 0) + kFeatureGain);
         if (real) {
           float *uo = a.u_out + mine * 512;
 #pragma unroll
           for (int oo = 0; oo < 2; ++oo)
 #pragma unroll
-            for (int b = 0; b < 8; ++b) uo[b * 64 + perm_orbit(lane + 32 * oo, perm_of(b))] = u[oo][b];
+            for (int b = 0; b < 8; ++b) uo[b * 64 + perm_orbit(lane + 32 * oo, perm_of(b))] = mul(sc, u[oo][b]);
         }
         if (a.target) {
           // folded (target - interpolation) / 8: the block-space target whose
@@ -256,8 +351,9 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
             for (int p = 0; p < 2; ++p)
 #pragma unroll
               for (int z = 1; z <= Cfg::MH; ++z) {
-                const int c = lane_cell(st, r, p, z);
-                scr[c] = sub(__ldg(tg + c), st.v[r][p][z]);
+                int cz, cy, cx;
+                lane_xyz(st, r, p, z, cz, cy, cx);
+                scr[scr_cell(cz, cy, cx)] = sub(__ldg(tg + (cz * 8 + cy) * 8 + cx), st.v[r][p][z]);
               }
           __syncwarp();
           float t[2][8];
@@ -273,7 +369,8 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
 #pragma unroll
             for (int oo = 0; oo < 2; ++oo)
 #pragma unroll
-              for (int b = 0; b < 8; ++b) to[b * 64 + perm_orbit(lane + 32 * oo, perm_of(b))] = mul(0.125f, t[oo][b]);
+              for (int b = 0; b < 8; ++b)
+                to[b * 64 + perm_orbit(lane + 32 * oo, perm_of(b))] = mul(sc, mul(0.125f, t[oo][b]));
           }
         }
         return;
@@ -284,14 +381,14 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
 #pragma unroll
           for (int b = 0; b < 8; ++b) {
             const int K = perm_orbit(lane + 32 * oo, perm_of(b));
-            const int row = side_of(b) * kWarps + warp;
-            __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(sB + group_of(b) * kGroupBytes) +
-                                 ((K >> 3) * kN + row) * 8 + (K & 7);
+            const int row = side_of(b) * kHalfWarps + wl;
+            __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(sB + group_of(b) * kGroupBytes +
+                                                                   (K >> 3) * kChunkB + row * 16) + (K & 7);
             *dst = __float2bfloat16_rn(u[oo][b]);
           }
         tc::fence_proxy_async_smem();
-        cta_bar();  // operands complete; the previous batch's results were read
-        if (tid == 0) {
+        half_bar(half);  // operands complete; the previous batch's results were read
+        if (wl == 0 && lane == 0) {
           tc::fence_after_sync();
           const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
 #pragma unroll
@@ -299,32 +396,33 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
 #pragma unroll
             for (int ks = 0; ks < kK / 16; ++ks) {
               const uint64_t ad = tc::smem_desc(a0 + (g ? kTileBytes : 0) + 2 * ks * 2048, 2048, 128);
-              const uint64_t bd = tc::smem_desc(b0 + g * kGroupBytes + 2 * ks * (kN * 16), kN * 16, 128);
+              const uint64_t bd = tc::smem_desc(b0 + g * kGroupBytes + 2 * ks * kChunkB, kChunkB, 128);
               tc::mma_bf16(tmem + uint32_t(g * kN), ad, bd, kIdesc, ks > 0 ? 1u : 0u);
             }
-          tc::mma_commit(&bars[0]);
+          tc::mma_commit(bar_mma);
         }
-        if (!tc::mbar_wait(&bars[0], phase, a.err)) late = true;
+        if (!tc::mbar_wait(bar_mma, phase, a.err)) late = true;
         last_parity = phase;
         phase ^= 1u;
         tc::fence_after_sync();
         // results: warp w reads TMEM lanes 32 (w % 4) .. + 31, i.e. class
-        // rows 32 (w & 1) .. of side (w & 3) >> 1, for groups w / 4 and w / 4 + 2
+        // rows 32 (w & 1) .. of side (w & 3) >> 1, for groups wl / 4 and wl / 4 + 2
         {
           const int q = warp & 3, side = q >> 1, row = 32 * (q & 1) + lane;
 #pragma unroll
           for (int gi = 0; gi < 2; ++gi) {
-            const int g = (warp >> 2) + 2 * gi;
+            const int g = (wl >> 2) + 2 * gi;
             float val[8];
-            tmem_ld8(tmem + (uint32_t(32 * q) << 16) + uint32_t(g * kN + side * kWarps), val);
+            tmem_ld8(tmem + (uint32_t(32 * q) << 16) + uint32_t(g * kN + side * kHalfWarps), val);
             tc::tmem_wait_ld();
             const int b = block_of(g, side), o = perm_orbit(row, perm_of(b));
+            float *dst = s_scr + size_t(half) * kHalfWarps * kScrWords + b * 64 + o;
 #pragma unroll
-            for (int n = 0; n < kWarps; ++n) s_scr[n * 512 + b * 64 + o] = val[n];
+            for (int n = 0; n < kHalfWarps; ++n) dst[n * kScrWords] = val[n];
           }
         }
         tc::fence_before_sync();
-        cta_bar();  // every team's block results are in its scratch
+        half_bar(half);  // every team's block results are in its scratch
         // unfold the own patch and add the correction to the start value
         float d[2][8];
 #pragma unroll
@@ -358,19 +456,21 @@ __global__ void __launch_bounds__(kThreads, 2) lin_sor_kernel(const LinArgs a) {
       SolveArgs<float> s = a.s;
       s.max_iter = 0;
       sor_solve_patch_with<float, 1, false, 2, 2>(s, P_, 0, lane, tb, false, hook);
+    } else if constexpr (kStaged) {
+      sor_solve_patch_with<float, 1, false, 2, 2, true>(a.s, P_, 0, lane, tb, real, hook, stg);
     } else {
       sor_solve_patch_with<float, 1, false, 2, 2>(a.s, P_, 0, lane, tb, real, hook);
     }
   }
   if constexpr (!FEATURES) {
-    // after a timed-out wait the MMAs may still run: wait for the last commit
-    // (bounded) before the accumulator columns are released
-    if (__syncthreads_or(late) && tid == 0) tc::mbar_wait(&bars[0], last_parity, a.err);
+    // after a timed-out wait the MMAs may still run: wait for the half's last
+    // commit (bounded) before the accumulator columns are released
+    if (__syncthreads_or(late) && wl == 0 && lane == 0 && it > 0) tc::mbar_wait(bar_mma, last_parity, a.err);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
       tc::fence_after_sync();
-      tc::tmem_dealloc(tmem, kTmemCols);
+      tc::tmem_dealloc(*s_tmem, kTmemCols);
     }
   }
 }

@@ -6,10 +6,12 @@
 // u[8][64] and, for training, the folded target t[8][64] = H(phi* - phi_i)/8,
 // phi* the converged solution; the prediction of block b is
 // v_b = W[class(b)] u_b with W[4][64][64] (row = output orbit, column = input
-// orbit, both in the class representative's axes).  Loss per training step:
-// mean over patches, blocks and rows of e^2 with e = s_p (v - t), s_p the
-// power of two that brings max|u_p| into [0.5, 1) -- a linear model is
-// indifferent to the scale, the loss is not.
+// orbit, both in the class representative's axes).  The features come scaled
+// by the power of two that brings the patch's max|phi_i| into [2^16, 2^17): a
+// linear model is indifferent to the scale, and the training loss, the mean
+// over patches, blocks and rows of e^2 with e = v - t, then measures each
+// patch's start error relative to its potential -- the quantity the solve is
+// judged by.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -64,35 +66,23 @@ __global__ void lin_pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__re
   }
 }
 
-// per patch (one CTA of 512 threads = 8 blocks x 64 rows): the scale s_p,
-// the scaled inputs us = s_p u and errors e = s_p (W u - t), and the patch's
-// sum of e^2 (fixed-order tree)
+// per patch (one CTA of 512 threads = 8 blocks x 64 rows): the errors
+// e = W u - t and the patch's sum of e^2 (fixed-order tree)
 __global__ void __launch_bounds__(512) lin_err_kernel(const float *__restrict__ u, const float *__restrict__ t,
-                                                      const float *__restrict__ w, float *__restrict__ us,
-                                                      float *__restrict__ e, float *__restrict__ loss_part) {
+                                                      const float *__restrict__ w, float *__restrict__ e,
+                                                      float *__restrict__ loss_part) {
   __shared__ float su[512];
   __shared__ float red[512];
   const int p = blockIdx.x, tid = threadIdx.x, b = tid >> 6, r = tid & 63;
-  const float x = u[int64_t(p) * 512 + tid];
-  su[tid] = x;
-  red[tid] = fabsf(x);
-  __syncthreads();
-  for (int h = 256; h > 0; h >>= 1) {
-    if (tid < h) red[tid] = fmaxf(red[tid], red[tid + h]);
-    __syncthreads();
-  }
-  int ex = 0;
-  frexpf(red[0], &ex);  // max|u| = m 2^ex, m in [0.5, 1)
-  const float s = red[0] > 0.f ? ldexpf(1.f, -ex) : 1.f;
+  su[tid] = u[int64_t(p) * 512 + tid];
   __syncthreads();
   const float *wr = w + (class_of(b) * kK + r) * kK;
   const float *ub = su + b * kK;
   float acc = 0.f;
 #pragma unroll 8
   for (int k = 0; k < kK; ++k) acc = fmaf(__ldg(wr + k), ub[k], acc);
-  const float err = s * (acc - t[int64_t(p) * 512 + tid]);
+  const float err = acc - t[int64_t(p) * 512 + tid];
   e[int64_t(p) * 512 + tid] = err;
-  us[int64_t(p) * 512 + tid] = s * x;
   red[tid] = err * err;
   __syncthreads();
   for (int h = 256; h > 0; h >>= 1) {
@@ -102,7 +92,7 @@ __global__ void __launch_bounds__(512) lin_err_kernel(const float *__restrict__ 
   if (tid == 0) loss_part[p] = red[0];
 }
 
-// grad[c][r][k] = 2 / (npatch 512) sum_p sum_{b in c} e[p][b][r] us[p][b][k]
+// grad[c][r][k] = 2 / (npatch 512) sum_p sum_{b in c} e[p][b][r] u[p][b][k]
 // (CTA = class c, 4 rows; thread = (row, k); patches and blocks in order)
 __global__ void __launch_bounds__(256) lin_grad_kernel(const float *__restrict__ us, const float *__restrict__ e,
                                                        int npatch, float *__restrict__ grad) {
@@ -138,10 +128,11 @@ struct gpg_lin {
   int step = 0;
   int probe_polls = 0;
   float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
-  float *us = nullptr, *e = nullptr, *loss_part = nullptr, *loss = nullptr;
+  float *e = nullptr, *loss_part = nullptr, *loss = nullptr;
   __nv_bfloat16 *tiles = nullptr;
   int *err = nullptr;
-  int grid = 0;  // persistent CTAs of the fused solve
+  int variant = 0;                   // launch shape of the fused solve
+  int grid[2] = {0, 0};              // persistent CTAs per shape (one per SM)
 };
 
 namespace {
@@ -152,21 +143,32 @@ int repack(gpg_lin *l, cudaStream_t s) {
   return GPG_OK;
 }
 
-template <bool FEATURES>
+// Launch shapes of the fused solve (identical results): 0 = two groups of 8
+// teams with staged inputs, 1 = three groups of 8 teams reading their inputs
+// from global memory.
+constexpr int kLinVariants = 2;
+
+template <bool FEATURES, int HALVES, bool STAGE>
 int prepare(int *grid) {
-  auto fn = gpg::lin::lin_sor_kernel<FEATURES>;
-  LIN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gpg::lin::Layout::bytes)));
+  auto fn = gpg::lin::lin_sor_kernel<FEATURES, HALVES, STAGE>;
+  using L = gpg::lin::Layout<HALVES, STAGE>;
+  LIN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
   LIN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 int(cudaSharedmemCarveoutMaxShared)));
   if (grid) {
-    int dev = 0, sms = 0, per = 0;
+    int dev = 0, sms = 0;
     LIN_CUDA(cudaGetDevice(&dev));
     LIN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    LIN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, gpg::lin::kThreads, gpg::lin::Layout::bytes));
-    if (per < 1) return lfail(GPG_ERR_UNSUPPORTED, "the fused kernel does not fit on an SM");
-    *grid = sms * per;
+    *grid = sms;  // one CTA per SM: its shared memory and TMEM take the whole SM
   }
   return GPG_OK;
+}
+
+// persistent CTAs for npatch patches: HALVES batches of 8 per CTA at a time
+int lin_grid(int halves, int grid_max, int npatch) {
+  const int64_t nbatch = (int64_t(npatch) + gpg::lin::kHalfWarps - 1) / gpg::lin::kHalfWarps;
+  const int64_t need = (nbatch + halves - 1) / halves;
+  return int(need < grid_max ? need : grid_max);
 }
 
 int check_solve_params(const gpg_params *p) {
@@ -211,7 +213,6 @@ extern "C" int gpg_lin_create(gpg_lin **out, int max_batch, int device_id) {
   al((void **)&l->adam_m, kParams * 4);
   al((void **)&l->adam_v, kParams * 4);
   al((void **)&l->tiles, 2 * gpg::lin::kTileBytes);
-  al((void **)&l->us, size_t(max_batch) * 512 * 4);
   al((void **)&l->e, size_t(max_batch) * 512 * 4);
   al((void **)&l->loss_part, size_t(max_batch) * 4);
   al((void **)&l->loss, 4);
@@ -225,11 +226,10 @@ extern "C" int gpg_lin_create(gpg_lin **out, int max_batch, int device_id) {
     return lfail(e == cudaErrorMemoryAllocation ? GPG_ERR_OOM : GPG_ERR_CUDA, "allocation: %s", cudaGetErrorString(e));
   }
   // attributes here, so that a stream capture never sees first-use set-up
-  if (int rc = prepare<false>(&l->grid)) {
-    gpg_lin_destroy(l);
-    return rc;
-  }
-  if (int rc = prepare<true>(nullptr)) {
+  int rc = prepare<false, 2, true>(&l->grid[0]);
+  if (!rc) rc = prepare<false, 3, false>(&l->grid[1]);
+  if (!rc) rc = prepare<true, 2, false>(nullptr);
+  if (rc) {
     gpg_lin_destroy(l);
     return rc;
   }
@@ -246,7 +246,7 @@ extern "C" int gpg_lin_destroy(gpg_lin *l) {
   if (!l) return GPG_OK;
   cudaSetDevice(l->device);
   for (void *p : {(void *)l->params, (void *)l->grad, (void *)l->adam_m, (void *)l->adam_v, (void *)l->tiles,
-                  (void *)l->us, (void *)l->e, (void *)l->loss_part, (void *)l->loss, (void *)l->err})
+                  (void *)l->e, (void *)l->loss_part, (void *)l->loss, (void *)l->err})
     cudaFree(p);
   delete l;
   return GPG_OK;
@@ -279,6 +279,9 @@ extern "C" int gpg_lin_solve_device(gpg_lin *l, const gpg_params *p, int npatch,
   if (npatch < 0) return lfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch == 0) return GPG_OK;
   if (!d_rho || !d_pot_in || !d_pot_out || (p->gra_acc && !d_flu)) return lfail(GPG_ERR_INVALID, "NULL array");
+  // the inputs are staged with bulk copies of whole patches
+  if ((reinterpret_cast<uintptr_t>(d_rho) | reinterpret_cast<uintptr_t>(d_pot_in)) & 15)
+    return lfail(GPG_ERR_INVALID, "d_rho and d_pot_in must be 16-byte aligned");
   gpg_params q = *p;
   q.init_mode = GPG_INIT_INTERP;  // the correction is added to the interpolated start
   gpg::lin::LinArgs a{};
@@ -286,10 +289,16 @@ extern "C" int gpg_lin_solve_device(gpg_lin *l, const gpg_params *p, int npatch,
   a.wtiles = l->tiles;
   a.err = l->err;
   a.probe_polls = l->probe_polls;
-  const int64_t nbatch = (int64_t(npatch) + gpg::lin::kWarps - 1) / gpg::lin::kWarps;
-  const int grid = int(nbatch < l->grid ? nbatch : l->grid);
-  gpg::lin::lin_sor_kernel<false>
-      <<<grid, gpg::lin::kThreads, gpg::lin::Layout::bytes, static_cast<cudaStream_t>(stream)>>>(a);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (l->variant == 0) {
+    using SH = gpg::lin::Shape<2, true>;
+    gpg::lin::lin_sor_kernel<false, 2, true><<<lin_grid(2, l->grid[0], npatch), SH::kThreads,
+                                               gpg::lin::Layout<2, true>::bytes, s>>>(a);
+  } else {
+    using SH = gpg::lin::Shape<3, false>;
+    gpg::lin::lin_sor_kernel<false, 3, false><<<lin_grid(3, l->grid[1], npatch), SH::kThreads,
+                                                gpg::lin::Layout<3, false>::bytes, s>>>(a);
+  }
   LIN_CUDA(cudaGetLastError());
   return GPG_OK;
 }
@@ -311,10 +320,9 @@ extern "C" int gpg_lin_features(gpg_lin *l, const gpg_params *p, int npatch, con
   a.t_out = d_t;
   a.target = d_target;
   a.err = l->err;
-  const int64_t nbatch = (int64_t(npatch) + gpg::lin::kWarps - 1) / gpg::lin::kWarps;
-  const int grid = int(nbatch < l->grid ? nbatch : l->grid);
-  gpg::lin::lin_sor_kernel<true>
-      <<<grid, gpg::lin::kThreads, gpg::lin::Layout::bytes, static_cast<cudaStream_t>(stream)>>>(a);
+  gpg::lin::lin_sor_kernel<true, 2, false>
+      <<<lin_grid(2, l->grid[0], npatch), gpg::lin::Shape<2, false>::kThreads, gpg::lin::Layout<2, false>::bytes,
+         static_cast<cudaStream_t>(stream)>>>(a);
   LIN_CUDA(cudaGetLastError());
   return GPG_OK;
 }
@@ -325,8 +333,8 @@ extern "C" int gpg_lin_gradients(gpg_lin *l, int npatch, const float *d_u, const
   if (npatch < 1 || npatch > l->max_batch) return lfail(GPG_ERR_INVALID, "npatch %d (1..%d)", npatch, l->max_batch);
   if (!d_u || !d_t) return lfail(GPG_ERR_INVALID, "NULL array");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  lin_err_kernel<<<npatch, 512, 0, s>>>(d_u, d_t, l->params, l->us, l->e, l->loss_part);
-  lin_grad_kernel<<<64, 256, 0, s>>>(l->us, l->e, npatch, d_grad ? d_grad : l->grad);
+  lin_err_kernel<<<npatch, 512, 0, s>>>(d_u, d_t, l->params, l->e, l->loss_part);
+  lin_grad_kernel<<<64, 256, 0, s>>>(d_u, l->e, npatch, d_grad ? d_grad : l->grad);
   lin_loss_kernel<<<1, 256, 0, s>>>(l->loss_part, npatch, d_loss ? d_loss : l->loss);
   LIN_CUDA(cudaGetLastError());
   return GPG_OK;
@@ -363,6 +371,15 @@ extern "C" int gpg_lin_check(gpg_lin *l) {
     LIN_CUDA(cudaMemset(l->err, 0, 4));
     return lfail(GPG_ERR_CUDA, "a tensor-core wait timed out");
   }
+  return GPG_OK;
+}
+
+extern "C" int gpg_lin_variant_count(void) { return kLinVariants; }
+
+extern "C" int gpg_lin_set_variant(gpg_lin *l, int variant) {
+  if (!l) return lfail(GPG_ERR_INVALID, "lin is NULL");
+  if (variant < 0 || variant >= kLinVariants) return lfail(GPG_ERR_INVALID, "variant %d", variant);
+  l->variant = variant;
   return GPG_OK;
 }
 

@@ -12,6 +12,8 @@
 // Operand order of every stencil follows the reference loops (bit-identical values).
 #pragma once
 
+#include <type_traits>
+
 #include <cfloat>
 
 #include "common.cuh"
@@ -272,14 +274,21 @@ __global__ void __launch_bounds__(NT) mg_kernel(const SolveArgs<T> a) {
     if (a.iters) a.iters[P] = iter;
     if (a.resid) a.resid[P] = err;
   }
-  {
-    const int GN = 8 + 2 * a.gra_ghost, shift = G - a.gra_ghost, GN3 = GN * GN * GN;
+  // output window, its edge a compile-time constant per GRA_GHOST_SIZE
+  auto window = [&](auto gg) {
+    constexpr int GG = decltype(gg)::value, GN = 8 + 2 * GG, shift = G - GG, GN3 = GN * GN * GN;
     T *dst = a.pot_out + P * GN3;
     for (int t = tid; t < GN3; t += NT) {
       const int i = t % GN, j = (t / GN) % GN, k = t / (GN * GN);
       dst[t] = s_sol[((k + shift) * N + (j + shift)) * N + (i + shift)];
     }
-  }
+  };
+  if (a.gra_ghost == 0)
+    window(std::integral_constant<int, 0>{});
+  else if (a.gra_ghost == 1)
+    window(std::integral_constant<int, 1>{});
+  else
+    window(std::integral_constant<int, 2>{});
   if (a.gra_acc) {
     gravity_patch<T, NT>(a.flu + P * 5 * 512, tid, a.gra_const, a.p5, [s_sol](int i, int j, int k) {
       return s_sol[((k + G) * N + (j + G)) * N + (i + G)];

@@ -37,10 +37,12 @@
 #pragma once
 
 #include <cfloat>
+#include <type_traits>
 
 #include "common.cuh"
 #include "gravity.cuh"
 #include "interp.cuh"
+#include "tc_common.cuh"
 
 namespace gpg {
 
@@ -344,10 +346,13 @@ struct SorLaneState {
 // start values and the stopping bound are set, before the first sweep; it
 // may change the interior (registers and shared cube) and must leave the
 // team synchronised.  store == false skips every global write (a team that
-// only keeps a CTA-wide schedule going).
-template <typename T, int G, bool PHASED, int Z, int Y, typename Hook>
+// only keeps a CTA-wide schedule going).  STAGED: the patch's coarse
+// potential and density come from `staged` in shared memory ([POT_NXT]^3
+// then [RHO_NXT]^3) instead of global memory.
+template <typename T, int G, bool PHASED, int Z, int Y, bool STAGED = false, typename Hook>
 __device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int64_t P_, int team, int tid,
-                                                     unsigned char *tb, bool store, Hook &&hook) {
+                                                     unsigned char *tb, bool store, Hook &&hook,
+                                                     const T *staged = nullptr) {
   using g = Geo<G>;
   using C = SorCfg<T, G, Z, Y>;
   using S = SorSmem<T, G, Z, Y>;
@@ -358,8 +363,8 @@ __device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int6
   double *s_part = reinterpret_cast<double *>(tb + S::round(S::cube_bytes));
 
   // ---- interpolate the coarse potential into the cube (reads via L1) -----
-  interpolate<T, G, TEAM>(a.pot_in + P_ * g::PN3, tid, a.int_scheme,
-                          [s_cube](int x, int y, int z, T v) { s_cube[C::addr(x, y, z)] = v; });
+  interpolate<T, G, TEAM, !STAGED>(STAGED ? staged : a.pot_in + P_ * g::PN3, tid, a.int_scheme,
+                                   [s_cube](int x, int y, int z, T v) { s_cube[C::addr(x, y, z)] = v; });
   team_sync<TEAM>(team);
 
   // ---- lane -> (rows, half, h) --------------------------------------------
@@ -388,7 +393,7 @@ __device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int6
   T crho[Y][2][MH];
   double cr_sum = 0.0;
   {
-    const T *rho = a.rho + P_ * g::RHO3;
+    const T *rho = STAGED ? staged + g::PN3 : a.rho + P_ * g::RHO3;
     const T *guess = a.guess ? a.guess + P_ * g::RHO3 : nullptr;
 #pragma unroll
     for (int rr = 0; rr < Y; ++rr) {
@@ -403,7 +408,12 @@ __device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int6
           const bool left = ((yr + z + c) & 1) == 0;
           const int x = left ? 2 * h + 1 : 2 * h + 2;
           const int idx = ((z - 1) * M + (yr - 1)) * M + (x - 1);
-          crho[rr][c][zz - 1] = active ? mul(a.sor_const, __ldg(rho + idx)) : T(0);
+          T rv = T(0);
+          if (active) {
+            if constexpr (STAGED) rv = rho[idx];
+            else rv = __ldg(rho + idx);
+          }
+          crho[rr][c][zz - 1] = active ? mul(a.sor_const, rv) : T(0);
           // tolerance scale: sum |Const rho| (mode 1) or sum |interpolated
           // phi| over the updated cells, before a start mode replaces it (3)
           cr_sum += (double)absval(a.stop_mode == 3 ? (active ? v[rr][c][zz] : T(0)) : crho[rr][c][zz - 1]);
@@ -492,14 +502,22 @@ __device__ __forceinline__ void sor_solve_patch_with(const SolveArgs<T> &a, int6
   }
 
   // ---- output window (CPU_PoissonSolver_SOR.cpp:305-311) ------------------
-  {
-    const int GN = 8 + 2 * a.gra_ghost, shift = G - a.gra_ghost, GN3 = GN * GN * GN;
+  // (edge GN a compile-time constant per GRA_GHOST_SIZE: the index split is
+  // then multiply-shift, not division)
+  auto window = [&](auto gg) {
+    constexpr int GG = decltype(gg)::value, GN = 8 + 2 * GG, shift = G - GG, GN3 = GN * GN * GN;
     T *dst = a.pot_out + P_ * GN3;
     for (int t = tid; t < GN3; t += TEAM) {
       const int i = t % GN, j = (t / GN) % GN, k = t / (GN * GN);
       dst[t] = s_cube[C::addr(i + shift, j + shift, k + shift)];
     }
-  }
+  };
+  if (a.gra_ghost == 0)
+    window(std::integral_constant<int, 0>{});
+  else if (a.gra_ghost == 1)
+    window(std::integral_constant<int, 1>{});
+  else
+    window(std::integral_constant<int, 2>{});
   // ---- fused gravity update (CPU_GravitySolver.cpp:34-79) -----------------
   if (a.gra_acc) {
     gravity_patch<T, TEAM>(a.flu + P_ * 5 * 512, tid, a.gra_const, a.p5,
@@ -529,6 +547,75 @@ __global__ void __launch_bounds__(PPC *SorCfg<T, G, Z, Y>::TEAM)
   const int64_t P_ = int64_t(blockIdx.x) * PPC + team;
   if (P_ >= a.npatch) return;  // whole team leaves together
   sor_solve_patch<T, G, PHASED, Z, Y>(a, P_, team, tid, smem_raw + team * SorSmem<T, G, Z, Y>::team_bytes);
+}
+
+// ---------------------------------------------------------------------------
+// Staged persistent variant: TPC teams per CTA, each team loops over patches
+// (team t of CTA c takes patches c*TPC + t, + gridDim.x*TPC, ...) and bulk-
+// copies its next patch's coarse potential and density into its shared
+// staging buffer while it solves the current one, so the interpolation and
+// the Const*rho loads read shared memory.  Same per-patch code as sor_kernel
+// (same bits).  A staging wait that gives up (about a second) leaves that
+// patch's iteration count at -1 and its residual NaN.
+// ---------------------------------------------------------------------------
+template <typename T, int G, int Z, int Y, int TPC>
+struct StagedSmem {
+  using S = SorSmem<T, G, Z, Y>;
+  static constexpr int stage_elems = Geo<G>::PN3 + Geo<G>::RHO3;
+  static constexpr size_t stage_bytes = S::round(sizeof(T) * stage_elems);
+  static constexpr size_t team_bytes = S::team_bytes + stage_bytes + 16;
+  static constexpr size_t bytes = TPC * team_bytes;
+  // CTAs that shared memory lets an SM hold (228 KB, 1 KB reserved per CTA);
+  // the register budget is bounded to match
+  static constexpr int ctas_per_sm = (228 * 1024) / (bytes + 1024) < 1    ? 1
+                                     : (228 * 1024) / (bytes + 1024) > 16 ? 16
+                                                                          : (228 * 1024) / (bytes + 1024);
+};
+
+template <typename T, int G, bool PHASED, int Z, int Y, int TPC>
+__global__ void __launch_bounds__(TPC *SorCfg<T, G, Z, Y>::TEAM, (StagedSmem<T, G, Z, Y, TPC>::ctas_per_sm))
+    staged_sor_kernel(const SolveArgs<T> a) {
+  using g = Geo<G>;
+  using SS = StagedSmem<T, G, Z, Y, TPC>;
+  constexpr int TEAM = SorCfg<T, G, Z, Y>::TEAM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int team = threadIdx.x / TEAM, tid = threadIdx.x - team * TEAM;
+  unsigned char *tb = smem_raw + team * SS::team_bytes;
+  T *stg = reinterpret_cast<T *>(tb + SS::S::team_bytes);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tb + SS::S::team_bytes + SS::stage_bytes);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_fence_init();
+  }
+  __syncthreads();
+  auto stage = [&](int64_t P) {  // one thread: patch P's inputs -> stg
+    tc::mbar_arrive_expect_tx(bar, uint32_t(sizeof(T) * SS::stage_elems));
+    tc::bulk_load(stg, a.pot_in + P * g::PN3, uint32_t(sizeof(T) * g::PN3), bar);
+    tc::bulk_load(stg + g::PN3, a.rho + P * g::RHO3, uint32_t(sizeof(T) * g::RHO3), bar);
+  };
+  const int64_t stride = int64_t(gridDim.x) * TPC;
+  int64_t P_ = int64_t(blockIdx.x) * TPC + team;
+  if (P_ < a.npatch && tid == 0) stage(P_);
+  uint32_t it = 0;
+  for (; P_ < a.npatch; P_ += stride, ++it) {
+    if (it) team_sync<TEAM>(team);  // the previous patch's output and gravity reads of the cube are done
+    const bool arrived = tc::mbar_wait(bar, it & 1u, nullptr);
+    const int64_t next = P_ + stride;
+    sor_solve_patch_with<T, G, PHASED, Z, Y, true>(
+        a, P_, team, tid, tb, true,
+        [&](const auto &) {
+          // the staged inputs are in the cube and registers: fetch the next patch
+          if (tid == 0 && next < a.npatch) {
+            tc::fence_proxy_async_smem();
+            stage(next);
+          }
+        },
+        stg);
+    if (!arrived && tid == 0) {
+      if (a.iters) a.iters[P_] = -1;
+      if (a.resid) a.resid[P_] = __longlong_as_double(0x7ff8000000000000ll);
+    }
+  }
 }
 
 }  // namespace gpg

@@ -121,6 +121,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return mbar_wait_polls(bar, parity, err, 1u << 26);
 }
 
+// --- bulk copies (TMA, one-dimensional, no multicast) ----------------------
+// The calling thread announces `bytes` of transaction on `bar` (one arrival);
+// each copy then completes its bytes on the barrier.  Source and destination
+// 16-byte aligned, sizes multiples of 16.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_global, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst_smem)),
+               "l"(src_global), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 // --- TMEM -> registers: 32 lanes x 16 columns of 32-bit per warp -----------
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];

@@ -35,6 +35,8 @@ def _lin_lib():
             "gpg_lin_apply_gradient": (C.c_int, [vp, vp, C.c_float, vp]),
             "gpg_lin_check": (C.c_int, [vp]),
             "gpg_lin_set_wait_probe": (C.c_int, [vp, C.c_int]),
+            "gpg_lin_variant_count": (C.c_int, []),
+            "gpg_lin_set_variant": (C.c_int, [vp, C.c_int]),
             "gpg_lin_last_error": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():
@@ -124,6 +126,14 @@ class LinearGuess:
         if grad.numel() != self.nparams or grad.dtype.itemsize != 4:
             raise ValueError(f"grad must be a float32 CUDA tensor of {self.nparams} values")
         _check(_lin_lib().gpg_lin_apply_gradient(self._l, _p(grad), lr, self._s(stream)))
+
+    def set_variant(self, variant: int):
+        """Launch shape of the fused solve (gpg_lin_set_variant); same results."""
+        _check(_lin_lib().gpg_lin_set_variant(self._l, int(variant)))
+
+    @staticmethod
+    def variant_count() -> int:
+        return int(_lin_lib().gpg_lin_variant_count())
 
     def set_wait_probe(self, polls: int):
         _check(_lin_lib().gpg_lin_set_wait_probe(self._l, int(polls)))

@@ -45,23 +45,26 @@ def patch_cost(ghost, expected_sweeps=None) -> np.ndarray:
     return cells * sweeps
 
 
-def scatter_solve_gather(arrays: dict, solve, group=None, src: int = 0) -> dict | None:
+def scatter_solve_gather(arrays: dict, solve, group=None, src: int = 0, cost=None) -> dict | None:
     """Rank `src` holds full host arrays ({name: ndarray [P, ...]}); every rank
     receives its contiguous slice, runs `solve(slices) -> {name: ndarray}`
     locally, and `src` gathers the outputs in patch order.  Point-to-point
-    transfers only; nothing is exchanged while ranks solve.  Returns the
-    gathered outputs on `src`, None elsewhere."""
+    transfers only; nothing is exchanged while ranks solve.  `cost` (on `src`:
+    an estimated cost per patch, e.g. patch_cost of a mixed-ghost batch)
+    balances the slices by cost instead of by count; `src` sends the bounds
+    to every rank.  Returns the gathered outputs on `src`, None elsewhere."""
     import torch
     import torch.distributed as dist
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     meta = [None]
     if rank == src:
         n = len(next(iter(arrays.values())))
-        meta = [{k: (v.shape, str(v.dtype)) for k, v in arrays.items()} | {"__n": n}]
+        meta = [{k: (v.shape, str(v.dtype)) for k, v in arrays.items()} |
+                {"__n": n, "__bounds": shard_bounds(n, world, cost)}]
     dist.broadcast_object_list(meta, src=src, group=group)
     meta = meta[0]
     n = meta.pop("__n")
-    bounds = shard_bounds(n, world)
+    bounds = meta.pop("__bounds")
     lo, hi = bounds[rank]
     local = {}
     for k, (shape, dt) in meta.items():

@@ -1,7 +1,7 @@
 """Train and evaluate the learned initial guesses for ghost-size-1 SOR.
 
     python gpu_testbed_poisson-gravity_b200/learned.py train --model lin --npatch 1048576 \
-        --out gpu_testbed_poisson-gravity_b200/weights/lin_correction
+        --epochs 64 --batch 2048 --lr 2e-3 --out gpu_testbed_poisson-gravity_b200/weights/lin_correction
     python gpu_testbed_poisson-gravity_b200/learned.py train --model conv --npatch 1048576 --epochs 2 \
         --out gpu_testbed_poisson-gravity_b200/weights/learned_init
     python gpu_testbed_poisson-gravity_b200/learned.py eval --npatch 65536
@@ -19,7 +19,8 @@ Two models, both trained on the GPU by the library's own kernels:
 Data: seeded ghost-1 patches (gpg.inputs) with rho0 log-uniform over 4
 decades and power index uniform in [1.5, 2.5].  Targets are the plain SOR's own
 solutions (reference rule from the interpolated start, i.e. converged to the
-FP32 round-off floor) computed by libgpg.  Evaluation solves held-out patches
+round-off floor) computed by libgpg: FP32 for the conv net, FP64 rounded to
+FP32 for the linear correction.  Evaluation solves held-out patches
 (other seeds) to the calibrated fixed residual (GPG_STOP_POT_TOLERANCE,
 gpg.abi.POT_TOL) from a zero start, from the interpolated start and from each
 learned start, and reports sweeps, patches/s (the model's cost included) and
@@ -296,9 +297,20 @@ def evaluate(net=None, lin=None, npatch: int = 65536, seed: int = 99, reps: int 
     return out
 
 
+def targets64(torch, rho, pin):
+    """The plain SOR's own FP64 solutions of the same (FP32) inputs: reference
+    rule from the interpolated start (converged to the FP64 round-off floor),
+    rounded once to FP32."""
+    p = default_params(8, 1, GPG_SOR, gra_acc=0, gra_ghost=0)
+    pot, _, _ = solve(torch, p, rho.double(), pin.double())
+    return pot.float()
+
+
 def lin_data(lin, rho, pin, chunk: int = CHUNK):
     """Training features (u, t) of ghost-1 patches: the folded residual of the
-    interpolated start and the folded correction to the plain SOR's solution."""
+    interpolated start and the folded correction to the plain SOR's FP64
+    solution (whose rounding error is far below that of an FP32 solve at its
+    floor, which would otherwise set the loss floor)."""
     import torch
     n = rho.shape[0]
     u = torch.empty((n, 8, 64), device=rho.device)
@@ -306,7 +318,7 @@ def lin_data(lin, rho, pin, chunk: int = CHUNK):
     p = sor_params(4, GPG_INIT_INTERP)
     for c0 in range(0, n, chunk):
         sl = slice(c0, min(n, c0 + chunk))
-        tg = targets(torch, rho[sl], pin[sl])
+        tg = targets64(torch, rho[sl], pin[sl])
         uu, tt = lin.features(p, rho[sl], pin[sl], target=tg)
         u[sl], t[sl] = uu, tt
     return u, t
@@ -419,9 +431,9 @@ def main(argv=None) -> int:
     t = sub.add_parser("train")
     t.add_argument("--model", choices=("conv", "lin"), default="conv")
     t.add_argument("--npatch", type=int, default=1 << 20)
-    t.add_argument("--epochs", type=int, default=None, help="default: conv 2, lin 4")
-    t.add_argument("--batch", type=int, default=1024)
-    t.add_argument("--lr", type=float, default=None, help="default: conv 2e-3, lin 1e-3")
+    t.add_argument("--epochs", type=int, default=None, help="default: conv 2, lin 64")
+    t.add_argument("--batch", type=int, default=None, help="default: conv 1024, lin 2048")
+    t.add_argument("--lr", type=float, default=None, help="default: conv 2e-3, lin 2e-3")
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--out", default=None, help="default: weights/learned_init (conv), weights/lin_correction (lin)")
     t.add_argument("--eval", type=int, default=65536, help="held-out patches evaluated after training (0: none)")
@@ -439,11 +451,12 @@ def main(argv=None) -> int:
         print(json.dumps(time_predict(a.npatch, a.reps, per_layer=not a.fused_only)))
     elif a.cmd == "train":
         conv = a.model == "conv"
-        epochs = a.epochs if a.epochs is not None else (2 if conv else 4)
-        lr = a.lr if a.lr is not None else (2e-3 if conv else 1e-3)
+        epochs = a.epochs if a.epochs is not None else (2 if conv else 64)
+        lr = a.lr if a.lr is not None else 2e-3
+        batch = a.batch if a.batch is not None else (1024 if conv else 2048)
         out = a.out if a.out is not None else (DEFAULT_WEIGHTS if conv else DEFAULT_LIN)
         fn = train if conv else train_lin
-        model, meta = fn(a.npatch, epochs, a.batch, lr, a.seed, out)
+        model, meta = fn(a.npatch, epochs, batch, lr, a.seed, out)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}))
             if a.eval:

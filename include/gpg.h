@@ -250,7 +250,13 @@ GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
  * lane): variants 0-5 give each lane a whole column of one row, 6-9 split the
  * column between two lanes (twice the threads, half the registers each),
  * 10-11 give a lane two rows and half a column, 12-13 two rows and a whole
- * column (not built where that exceeds the register file: GPG_ERR_UNSUPPORTED).
+ * column (not built where that exceeds the register file: GPG_ERR_UNSUPPORTED);
+ * 14-16 run the layouts of 10, 11 and 13 in a staged persistent kernel: each
+ * team loops over patches and bulk-copies its next patch's coarse potential
+ * and density into shared memory while it solves the current one (patches per
+ * CTA reported as 0; inputs that are not 16-byte aligned run unstaged; a
+ * staging wait that gives up after about a second leaves that patch's
+ * iteration count at -1 and its residual NaN).
  * Variants 0-5 return identical bits; the others sum the residual in another
  * order, so a stop decision can differ only where two sweeps' totals tie.  The table starts from the library's defaults, then an optional
  * tuning file ($GPG_TUNE_FILE, else sor_tune.txt beside libgpg.so, lines
@@ -259,6 +265,7 @@ GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
 GPG_API int gpg_sor_variant_count(void);
 GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased);
 GPG_API int gpg_sor_variant_layout(int variant, int *lanes_per_column, int *rows_per_lane);
+GPG_API int gpg_sor_variant_staged(int variant, int *staged);
 /* The lane layout a variant uses at (real_size, ghost), for tools and tests
  * that check its indexing on the host: fields[GPG_SOR_LAYOUT_FIELDS] =
  * {lanes per column Z, rows per lane Y, heights per lane MH, lanes per row R,
@@ -349,12 +356,15 @@ GPG_API int gpg_lin_solve_device(gpg_lin *lin, const gpg_params *p, int npatch, 
  * each patch (block b at b*64, orbit index in its class's axes); when
  * d_target [P][8]^3 (a converged interior potential) is given, d_t [P][8][64]
  * the folded (target - interpolated start) / 8, so that the unfold of
- * W u ~ t is the correction. */
+ * W u ~ t is the correction.  Both are scaled by the power of two 2^(17 - e)
+ * with the patch's largest |interpolated potential| = m 2^e, m in [0.5, 1):
+ * exact, immaterial to a linear map; it makes the training loss measure each
+ * patch's start error relative to its potential, with the features near one. */
 GPG_API int gpg_lin_features(gpg_lin *lin, const gpg_params *p, int npatch, const float *d_rho,
                              const float *d_pot_in, const float *d_target, float *d_u, float *d_t, void *stream);
-/* loss = mean over patches, blocks and rows of (s_p (W u - t))^2, s_p the
- * power of two with max|u_p| s_p in [0.5, 1); its gradient wrt W into d_grad
- * [16384] (may be NULL: kept inside) and the loss into d_loss (may be NULL) */
+/* loss = mean over patches, blocks and rows of (W u - t)^2; its gradient wrt
+ * W into d_grad [16384] (may be NULL: kept inside) and the loss into d_loss
+ * (may be NULL) */
 GPG_API int gpg_lin_gradients(gpg_lin *lin, int npatch, const float *d_u, const float *d_t, float *d_grad,
                               float *d_loss, void *stream);
 /* gradients + one Adam step (beta 0.9 / 0.999, eps 1e-8) */
@@ -362,6 +372,12 @@ GPG_API int gpg_lin_train_step(gpg_lin *lin, int npatch, const float *d_u, const
                                float *d_loss, void *stream);
 /* one Adam step with a caller-supplied gradient (data-parallel training) */
 GPG_API int gpg_lin_apply_gradient(gpg_lin *lin, const float *d_grad, float lr, void *stream);
+/* Launch shape of the fused solve: 0 (default) = per SM two groups of 8 teams
+ * whose inputs are prefetched into shared memory by bulk copies, 1 = three
+ * groups of 8 teams reading their inputs from global memory.  Every shape
+ * gives the same bits. */
+GPG_API int gpg_lin_variant_count(void);
+GPG_API int gpg_lin_set_variant(gpg_lin *lin, int variant);
 /* GPG_ERR_CUDA when a tensor-core wait of an earlier solve timed out; reading
  * the flag clears it */
 GPG_API int gpg_lin_check(gpg_lin *lin);

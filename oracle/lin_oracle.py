@@ -11,7 +11,9 @@ interp_cube) and the SOR residual expression (CPU_PoissonSolver_SOR.cpp:
 * ``apply``      block b times W[class(b)] with BF16 operands (FP64 sums here;
                  the tensor cores sum in FP32), then the unfold (FP32) and
                  the FP32 add to the interpolated start;
-* ``targets``    the folded (target - start) / 8 of the training features;
+* ``features``   the training input: the folded residual, scaled by the
+                 power of two of the patch's largest interpolated potential;
+* ``targets``    the folded (target - start) / 8, scaled the same way;
 * ``gradients``  the training loss and its gradient (FP64).
 
 ``green_params`` gives the exact correction: the block form of minus the
@@ -132,30 +134,44 @@ def learned_start(w, cube, rho, cnst):
     return (interior + d).reshape(-1, 8, 8, 8)
 
 
+FEATURE_GAIN = 17
+
+
+def feature_scale(cube):
+    """[P] the power of two 2^(17 - e) with max|interpolated interior| = m 2^e,
+    m in [0.5, 1) (e = 0 for an all-zero interior), FP32."""
+    m = np.abs(np.asarray(cube, dtype=np.float32)[:, 1:-1, 1:-1, 1:-1]).reshape(len(cube), -1).max(1)
+    ex = np.where(m > 0, np.frexp(m.astype(np.float64))[1], 0)
+    return np.ldexp(1.0, FEATURE_GAIN - ex).astype(np.float32)
+
+
+def features(cube, rho, cnst):
+    """The training input u [P][8][64]: the folded residual, scaled."""
+    return feature_scale(cube)[:, None, None] * fold(residual(cube, rho, cnst))
+
+
 def targets(cube, target):
-    """Folded (target - interpolated interior) / 8 [P][8][64] (FP32)."""
+    """The training target t [P][8][64]: folded (target - interpolated
+    interior) / 8, scaled like the features (FP32)."""
     interior = np.asarray(cube, dtype=np.float32)[:, 1:-1, 1:-1, 1:-1].reshape(-1, 512)
     d = np.asarray(target, dtype=np.float32).reshape(-1, 512) - interior
-    return np.float32(0.125) * fold(d)
+    return feature_scale(cube)[:, None, None] * (np.float32(0.125) * fold(d))
 
 
 def gradients(w, u, t):
-    """(loss, grad [4][64][64]) in FP64 of the training objective."""
+    """(loss, grad [4][64][64]) in FP64 of the training objective: the mean of
+    e^2 over patches, blocks and rows, e = W[class] u - t."""
     w = np.asarray(w, dtype=np.float64).reshape(4, K, K)
     u = np.asarray(u, dtype=np.float64)
     t = np.asarray(t, dtype=np.float64)
-    m = np.abs(u).reshape(u.shape[0], -1).max(1)
-    ex = np.frexp(m)[1]
-    s = np.where(m > 0, np.ldexp(1.0, -ex), 1.0)[:, None, None]
     v = np.empty_like(u)
     for b in range(8):
         v[:, b] = u[:, b] @ w[class_of(b)].T
-    e = s * (v - t)
-    us = s * u
+    e = v - t
     n = u.shape[0] * 512
     grad = np.zeros((4, K, K))
     for b in range(8):
-        grad[class_of(b)] += e[:, b].T @ us[:, b]
+        grad[class_of(b)] += e[:, b].T @ u[:, b]
     return float((e ** 2).sum() / n), grad * (2.0 / n)
 
 

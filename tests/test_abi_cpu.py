@@ -76,17 +76,20 @@ def test_device_call_without_gpu_reports_error():
 
 
 def test_sor_variant_table_queries():
-    """The variant table answers without a GPU: 14 launch shapes, each with a
-    CTA size, pass order and layout; out-of-range ids are rejected."""
+    """The variant table answers without a GPU: 17 launch shapes, each with a
+    CTA size (0: staged persistent), pass order and layout; out-of-range ids
+    are rejected."""
     lib = library()
     n = lib.gpg_sor_variant_count()
-    assert n == 14
+    assert n == 17
     shapes = set()
     for v in range(n):
-        ppc, ph, z, y = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ppc, ph, z, y, st = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
         check(lib.gpg_sor_variant_info(v, C.byref(ppc), C.byref(ph)))
         check(lib.gpg_sor_variant_layout(v, C.byref(z), C.byref(y)))
-        assert ppc.value in (1, 2, 4) and ph.value in (0, 1) and z.value in (1, 2) and y.value in (1, 2)
+        check(lib.gpg_sor_variant_staged(v, C.byref(st)))
+        assert ph.value in (0, 1) and z.value in (1, 2) and y.value in (1, 2)
+        assert (ppc.value == 0) == bool(st.value) and ppc.value in (0, 1, 2, 4)
         shapes.add((ppc.value, ph.value, z.value, y.value))
     assert len(shapes) == n  # no two variants alike
     for bad in (-1, n):

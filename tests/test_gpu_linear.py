@@ -63,7 +63,7 @@ def test_features_bit_identical_to_oracle(torch, lin):
                         target=torch.from_numpy(target).cuda())
     torch.cuda.synchronize()
     cubes = _cubes(d["pot_in"])
-    want_u = lo.fold(lo.residual(cubes, d["rho"], CNST))
+    want_u = lo.features(cubes, d["rho"], CNST)
     want_t = lo.targets(cubes, target)
     assert np.array_equal(u.cpu().numpy(), want_u)
     assert np.array_equal(t.cpu().numpy(), want_t)
@@ -158,26 +158,29 @@ def test_gradients_match_oracle(torch, lin):
 
 
 def test_training_recovers_the_correction(torch, lin):
-    """A short training run on the plain SOR's own solutions drives the loss
-    down and moves W towards the exact correction (the inverse Laplacian)."""
+    """A short training run on the plain SOR's own FP64 solutions drives the
+    loss down and W towards the exact correction (minus the inverse
+    Laplacian of the interior, block form)."""
     import learned
     from gpg.linear import LinearGuess
     from oracle.lin_oracle import green_params
-    m = LinearGuess(max_batch=512)
+    m = LinearGuess(max_batch=1024)
     rho, pin = learned.dataset(16384, 21)
     u, t = learned.lin_data(m, torch.from_numpy(rho).cuda(), torch.from_numpy(pin).cuda())
     loss = torch.empty(1, device="cuda")
     first = None
-    for step in range(600):
-        sl = slice((step % 32) * 512, (step % 32 + 1) * 512)
-        m.train_step(u[sl], t[sl], 2e-3 * 0.5 * (1 + np.cos(np.pi * step / 600)), loss=loss)
+    nstep = 1500
+    for step in range(nstep):
+        sl = slice((step % 16) * 1024, (step % 16 + 1) * 1024)
+        m.train_step(u[sl], t[sl], 2e-3 * 0.5 * (1 + np.cos(np.pi * step / nstep)), loss=loss)
         if step == 0:
             first = loss.item()
+    m.gradients(u[:1024], t[:1024], loss=loss)
     last = loss.item()
-    assert last < 0.05 * first, (first, last)
+    assert last < 0.02 * first, (first, last)
     w = m.params().reshape(4, 64, 64).astype(np.float64)
     g = green_params()
-    assert np.linalg.norm(w - g) < 0.5 * np.linalg.norm(g)
+    assert np.linalg.norm(w - g) < 0.1 * np.linalg.norm(g), np.linalg.norm(w - g) / np.linalg.norm(g)
     # held-out patches: the learned start is far closer to the FP64 solution
     # than the interpolated start it corrects
     from gpg.lib import solve_device
@@ -226,3 +229,44 @@ def test_rejects_other_shapes(torch, lin):
         p = default_params(kw.get("real_size", 4), kw.get("ghost", 1), GPG_SOR)
         with pytest.raises(GpgError):
             lin.solve(p, rho, pin)
+
+
+def test_launch_shapes_give_the_same_bits(torch, lin):
+    """Every launch shape of the fused solve (staged or not, 2 or 3 groups of
+    teams per SM) computes each patch the same way: identical results."""
+    lin.set_params(_green())
+    d = _patches(203, 31)
+    rho, pin = torch.from_numpy(d["rho"]).cuda(), torch.from_numpy(d["pot_in"]).cuda()
+    p = fixed_residual_params(4, 1)
+    outs = []
+    try:
+        for v in range(lin.variant_count()):
+            lin.set_variant(v)
+            pot, _, it, rs = lin.solve(p, rho, pin)
+            torch.cuda.synchronize()
+            lin.check()
+            outs.append((pot.clone(), it.clone(), rs.clone()))
+    finally:
+        lin.set_variant(0)
+    assert len(outs) >= 2
+    for o in outs[1:]:
+        assert all(torch.equal(a, b) for a, b in zip(o, outs[0]))
+
+
+def test_trained_correction_doubles_throughput(torch):
+    """The committed checkpoint on held-out patches, every start to the same
+    calibrated fixed residual: the learned start reaches it with at least twice
+    the patches/s of the zero-start plain SOR, in fewer sweeps than the
+    interpolated start, with the FP64 error of the zero start or better (median;
+    the maximum within 25 % of it and inside the 1e-5 FP32 bound)."""
+    import learned
+    from gpg.linear import LinearGuess
+    lin = LinearGuess(max_batch=1)
+    learned.load_lin(lin)
+    r = learned.evaluate(lin=lin, npatch=32768, seed=77, reps=10, rule=False)
+    lin.close()
+    z, i, l = r["plain_zero_start"], r["plain_interpolated_start"], r["learned_linear"]
+    assert l["patches_per_s"] >= 2.0 * z["patches_per_s"], r
+    assert l["sweeps"]["mean"] < 0.5 * i["sweeps"]["mean"] and i["sweeps"]["mean"] < z["sweeps"]["mean"], r
+    assert l["rel_linf_vs_fp64"]["p50"] <= z["rel_linf_vs_fp64"]["p50"], r
+    assert l["rel_linf_vs_fp64"]["max"] <= 1.25 * z["rel_linf_vs_fp64"]["max"] and l["rel_linf_vs_fp64"]["max"] < 1e-5, r

@@ -85,6 +85,74 @@ def test_scatter_solve_gather_gloo_world2():
     assert q.get(timeout=5) is True
 
 
+def _mixed_worker(rank, world, port, q):
+    """A mixed-ghost batch (each patch's arrays padded to the largest shape)
+    split by cost: ranks get unequal patch counts and the gathered result is
+    the single-process one."""
+    import datetime
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.dirname(here))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "gpu_testbed_poisson-gravity_b200"))
+    import torch.distributed as dist
+    from gpg.abi import GPG_SOR, default_params
+    from gpg.inputs import make_patches
+    from gpg.shard import patch_cost, scatter_solve_gather
+    from oracle.oracle import run_oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    ghosts = np.array([1] * 12 + [5] * 4 + [3] * 8, dtype=np.int32)
+    arrays, cost = None, None
+    if rank == 0:
+        rho = np.zeros((len(ghosts), 16 ** 3), np.float32)
+        pin = np.zeros((len(ghosts), 12 ** 3), np.float32)
+        for i, g in enumerate(ghosts):
+            d = make_patches(1, int(g), seed=40 + i, fluid=False)
+            rho[i, :d["rho"].size] = d["rho"].reshape(-1)
+            pin[i, :d["pot_in"].size] = d["pot_in"].reshape(-1)
+        arrays = {"ghost": ghosts, "rho": rho, "pot_in": pin}
+        cost = patch_cost(ghosts)
+
+    def solve_one(g, rho, pin):
+        m, pn = 6 + 2 * g, 4 + 2 * ((g + 3) // 2)
+        p = default_params(4, g, GPG_SOR, gra_acc=0, gra_ghost=0)
+        pot, _, it, _ = run_oracle(p, np.ascontiguousarray(rho[:, :m ** 3].reshape(-1, m, m, m)),
+                                   np.ascontiguousarray(pin[:, :pn ** 3].reshape(-1, pn, pn, pn)))
+        return pot.reshape(len(rho), -1)[:, :512], it
+
+    def solve(local):
+        pots = np.zeros((len(local["ghost"]), 512), np.float32)
+        its = np.zeros(len(local["ghost"]), np.int32)
+        for g in np.unique(local["ghost"]):
+            sel = local["ghost"] == g
+            pots[sel], its[sel] = solve_one(int(g), local["rho"][sel], local["pot_in"][sel])
+        return {"pot": pots, "iters": its, "count": np.full(len(its), len(its), np.int32)}
+
+    out = scatter_solve_gather(arrays, solve, cost=cost)
+    if rank == 0:
+        want = solve({"ghost": ghosts, "rho": arrays["rho"], "pot_in": arrays["pot_in"]})
+        counts = sorted(set(out["count"].tolist()))
+        q.put(bool(np.array_equal(out["pot"], want["pot"]) and np.array_equal(out["iters"], want["iters"])
+                   and len(counts) == 2))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_cost_balanced_scatter_gloo_world2():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mixed_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(timeout=120)
+    assert all(pr.exitcode == 0 for pr in procs)
+    assert q.get(timeout=5) is True
+
+
 def _mean_worker(rank, world, port, q):
     import datetime
     import sys
