@@ -27,7 +27,10 @@ def test_reference_arm_line():
         assert k in d, k
     assert d["impl"] == "reference" and d["n_gpus"] == 1 and d["steps"] == 1
     assert d["unit"] == "patches/s" and d["higher_is_better"] is True and d["value"] > 0
-    assert d["config"]["global_batch"] == 32768
+    sys.path.insert(0, REPO)
+    import bench
+    assert d["config"] == bench.bench_config()  # the same dict as the GPU arm's
+    assert d["config"]["patches_per_gpu_per_step"] == 32768
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "patches/s", "h2d_bytes_per_step": 0,
