@@ -141,15 +141,30 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference CPU path
 # ---------------------------------------------------------------------------
+_HOST_THREADS = 0
+
+
+def host_threads() -> int:
+    """All OpenMP threads of the host, read once before any run narrows them
+    (the reference's CPU objects share one OpenMP runtime: a one-core run
+    would otherwise leave every later call on one thread)."""
+    global _HOST_THREADS
+    if not _HOST_THREADS:
+        from oracle.oracle import oracle_lib
+        _HOST_THREADS = max(1, oracle_lib().oracle_max_threads())
+    return _HOST_THREADS
+
+
 def reference_cpu(batches, budget_s: float = 20.0, nthreads: int = 0, keep: dict | None = None):
     """Time the reference's CPU_PoissonGravitySolver (oracle/_ref; the C port
     of oracle/ when the reference objects are absent) on a bounded sample of
     every batch.  Returns (patches/s, cores, kind, sample description); `keep`
     receives {batch index: (patch indices, potential)} of the timed runs."""
-    from oracle.oracle import oracle_lib, ref_available, run_oracle, run_reference
+    from oracle.oracle import ref_available, run_oracle, run_reference
     kind = "reference" if all(ref_available("sor", p.ghost, 1, "f32" if p.real_size == 4 else "f64")
                               for p, _ in batches) else "port"
-    cores = nthreads or (oracle_lib().oracle_max_threads())
+    cores = nthreads or host_threads()
+    nthreads = cores
     # per batch sample: n patches spread over the batch, sized from a probe run
     total_t, total_p, desc = 0.0, 0, []
     per_batch = budget_s / len(batches)
@@ -264,7 +279,7 @@ def extra_configs(torch, dev, cpu: bool):
     rec["errors"] = {"pot_vs_fp64": rel_linf(gpot, pot64.cpu().numpy()),
                      "flu_vs_fp64": rel_linf(gflu, flu64.cpu().numpy())}
     if cpu:
-        from oracle.oracle import oracle_lib, ref_available, run_reference
+        from oracle.oracle import ref_available, run_reference
         if ref_available("mg", 3, 2, "f32"):
             # 4096 patches spread over the batch, all host threads, a warm-up
             # call and the best of 3 timed calls
@@ -275,11 +290,11 @@ def extra_configs(torch, dev, cpu: bool):
             for r in range(4):
                 pin_c, flu_c = sub["pot_in"].copy(), sub["flu"].copy()
                 t0 = time.perf_counter()
-                rpot, rflu, _ = run_reference(p, sub["rho"], pin_c, flu=flu_c)
+                rpot, rflu, _ = run_reference(p, sub["rho"], pin_c, flu=flu_c, nthreads=host_threads())
                 dt = time.perf_counter() - t0
                 if r > 0:
                     best = dt if best is None else min(best, dt)
-            rec["cpu_reference"] = {"patches_per_s": m / best, "cores": oracle_lib().oracle_max_threads(),
+            rec["cpu_reference"] = {"patches_per_s": m / best, "cores": host_threads(),
                                     "sample": f"{m} patches spread over the batch, warm-up + best of 3"}
             rec["errors"]["pot_vs_reference_cpu"] = rel_linf(gpot[idx], rpot)
             rec["errors"]["flu_vs_reference_cpu"] = rel_linf(gflu[idx], rflu)
@@ -414,19 +429,20 @@ def default_case(torch, dev, cpu: bool) -> dict:
     rec = {"workload": "256 patches, ghost 1, FP32, SOR reference rule + gravity (the reference's default run)",
            "ms": ms, "patches_per_s": n / ms * 1e3, "timing": "device-resident, CUDA events, mean of 50 calls"}
     if cpu:
-        from oracle.oracle import oracle_lib, ref_available, run_reference
+        from oracle.oracle import ref_available, run_reference
         if ref_available("sor", 1, 1, "f32"):
             best = None
             for r in range(4):
                 t0 = time.perf_counter()
-                rpot, rflu, _ = run_reference(p, d["rho"], d["pot_in"].copy(), flu=d["flu"].copy())
+                rpot, rflu, _ = run_reference(p, d["rho"], d["pot_in"].copy(), flu=d["flu"].copy(),
+                                              nthreads=host_threads())
                 dt = time.perf_counter() - t0
                 if r > 0:
                     best = dt if best is None else min(best, dt)
             flu1 = t["flu"].clone()
             solve_device(p, t["rho"], t["pot_in"], pot_out=pot, flu=flu1)
             rec["cpu_reference"] = {"ms": best * 1e3, "patches_per_s": n / best,
-                                    "cores": oracle_lib().oracle_max_threads(), "sample": "all 256, warm-up + best of 3"}
+                                    "cores": host_threads(), "sample": "all 256, warm-up + best of 3"}
             rec["errors"] = {"pot_vs_reference_cpu": rel_linf(pot.cpu().numpy(), rpot),
                              "flu_vs_reference_cpu": rel_linf(flu1.cpu().numpy(), rflu)}
     return rec

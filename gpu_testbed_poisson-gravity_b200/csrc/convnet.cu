@@ -320,6 +320,7 @@ int launch_wgrad(const WgradArgs &a, int grid, cudaStream_t s) {
 struct gpg_net {
   int device = 0;
   int max_batch = 0;
+  int probe_polls = 0;  // test hook of the inference kernel (gpg_net_set_wait_probe)
   int64_t step = 0;
   float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   __nv_bfloat16 *wf[kLayers] = {}, *wb[kLayers] = {};
@@ -565,7 +566,17 @@ extern "C" int gpg_net_check(gpg_net *n) {
   if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
   int flag = 0;
   NET_CUDA(cudaMemcpy(&flag, n->err, 4, cudaMemcpyDeviceToHost));
-  if (flag) return nfail(GPG_ERR_CUDA, "a tensor-core wait timed out");
+  if (flag) {
+    NET_CUDA(cudaMemset(n->err, 0, 4));  // reported once
+    return nfail(GPG_ERR_CUDA, "a tensor-core wait timed out");
+  }
+  return GPG_OK;
+}
+
+extern "C" int gpg_net_set_wait_probe(gpg_net *n, int polls) {
+  if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
+  if (polls < 0) return nfail(GPG_ERR_INVALID, "polls %d", polls);
+  n->probe_polls = polls;
   return GPG_OK;
 }
 
@@ -589,6 +600,7 @@ extern "C" int gpg_net_predict(gpg_net *n, int npatch, const float *d_rho, const
   }
   a.cnst = float(cnst);
   a.npatch = npatch;
+  a.probe_polls = n->probe_polls;
   a.err = n->err;
   const int grid = std::min(npatch, sm_count());  // persistent: one CTA per SM (shared memory bound)
   gpg::net::net_infer_kernel<<<grid, gpg::net::kInferThreads, InferSmem::bytes, s>>>(a);

@@ -91,11 +91,12 @@ struct InferSmem {
   static constexpr uint32_t tmem_slot = bars + (2 * kRing + 1) * 8;
   static constexpr uint32_t red = tmem_slot + 16;              // one float per compute warp
   static constexpr uint32_t flag = red + 4 * (kComputeThreads / 32);  // abort flag
+  static constexpr uint32_t probe = flag + 8;                  // test-hook barrier (never signalled)
   static constexpr uint32_t ring = (flag + 16 + 1023u) & ~1023u;
   static constexpr uint32_t bytes = ring + kRing * kSlotBytes;
 };
 static_assert(InferSmem::bytes <= 232448, "shared memory per CTA");
-static_assert(InferSmem::bars % 8 == 0, "mbarrier alignment");
+static_assert(InferSmem::bars % 8 == 0 && InferSmem::probe % 8 == 0, "mbarrier alignment");
 // the farthest descriptor read: buffer B, chunk 3, rows up to 133 + 128*9 + 133 + 127 = 1545
 static_assert(InferSmem::buf_b + 3 * kChunkBytes + (kRowCube + 128 * kTilesCube + kMaxOffset) * 16 <= kChainBytes,
               "shifted tile reads stay inside the activation chain");
@@ -114,6 +115,7 @@ struct InferArgs {
   float cnst;                    // Poi_Coeff * dh^2
   int64_t npatch;
   int *err;
+  int probe_polls;               // > 0: thread 0 also waits that many polls on a barrier nothing signals
 };
 
 __host__ __device__ constexpr int tap_offset(int t) {
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(accb, 1);
+    tc::mbar_init(reinterpret_cast<uint64_t *>(smem + S::probe), 1);
     *s_abort = 0;
     tc::mbar_fence_init();
   }
@@ -235,6 +238,11 @@ __global__ void __launch_bounds__(kInferThreads, 1) net_infer_kernel(const Infer
   tc::fence_before_sync();
   __syncthreads();  // the last barrier all 9 warps take
   tc::fence_after_sync();
+  if (a.probe_polls > 0 && tid == 0) {
+    // test hook: a bounded wait on a barrier nothing arrives on gives up
+    // after probe_polls polls, records the timeout and the kernel goes on
+    tc::mbar_wait_polls(reinterpret_cast<uint64_t *>(smem + S::probe), 0, a.err, uint32_t(a.probe_polls));
+  }
 
   const int64_t my_patches = a.npatch > blockIdx.x ? (a.npatch - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int64_t total_units = my_patches * kUnitsPerPatch;

@@ -26,6 +26,7 @@ def _net_lib():
             "gpg_net_train_step": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, C.c_float, vp, vp]),
             "gpg_net_apply_gradient": (C.c_int, [vp, vp, C.c_float, vp]),
             "gpg_net_check": (C.c_int, [vp]),
+            "gpg_net_set_wait_probe": (C.c_int, [vp, C.c_int]),
             "gpg_net_last_error": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():
@@ -108,6 +109,10 @@ class Net:
 
     def check(self):
         _check(_net_lib().gpg_net_check(self._n))
+
+    def set_wait_probe(self, polls: int):
+        """Test hook (gpg_net_set_wait_probe)."""
+        _check(_net_lib().gpg_net_set_wait_probe(self._n, int(polls)))
 
     def close(self):
         if self._n:

@@ -316,8 +316,13 @@ GPG_API int gpg_net_train_step(gpg_net *net, int npatch, const float *d_rho, con
  * gpg_net_gradients, averages them across ranks (an all-reduce), and applies
  * the average here on every rank; gradients + this call = gpg_net_train_step */
 GPG_API int gpg_net_apply_gradient(gpg_net *net, const float *d_grad, float lr, void *stream);
-/* GPG_ERR_CUDA when a tensor-core wait timed out in an earlier call */
+/* GPG_ERR_CUDA when a tensor-core wait timed out in an earlier call; reading
+ * the flag clears it */
 GPG_API int gpg_net_check(gpg_net *net);
+/* Test hook: with polls > 0 every later gpg_net_predict also makes one
+ * bounded wait of that many polls on a barrier nothing signals, so the
+ * timeout path runs (the prediction itself completes normally); 0 = off. */
+GPG_API int gpg_net_set_wait_probe(gpg_net *net, int polls);
 GPG_API const char *gpg_net_last_error(void);
 
 /* ---------------------------------------------------------------------------

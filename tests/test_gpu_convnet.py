@@ -272,3 +272,33 @@ def test_data_parallel_training_under_torchrun(torch, tmp_path):
     w1 = np.fromfile(str(tmp_path / "single.bin"), dtype=np.float32)
     w2 = np.fromfile(str(tmp_path / "dp.bin"), dtype=np.float32)
     assert w1.size == w2.size and np.array_equal(w1, w2)
+
+
+def test_bounded_wait_reports_timeout_and_recovers(torch):
+    """The inference kernel's bounded tensor-core wait: a wait on a barrier
+    nothing signals gives up after a few polls, every thread leaves through
+    the normal path (the prediction is unchanged), gpg_net_check reports
+    GPG_ERR_CUDA once, and the next call is clean."""
+    from gpg.lib import GpgError
+    from gpg.net import Net
+    rho, pin, _ = _data(24, 5)
+    rho, pin = torch.from_numpy(rho).cuda(), torch.from_numpy(pin).cuda()
+    net = Net(max_batch=32, seed=2)
+    ref = torch.empty((24, 8, 8, 8), device="cuda")
+    net.predict(rho, pin, ref, float(CNST))
+    torch.cuda.synchronize()
+    net.check()
+    net.set_wait_probe(4)
+    got = torch.empty_like(ref)
+    net.predict(rho, pin, got, float(CNST))
+    torch.cuda.synchronize()
+    with pytest.raises(GpgError) as ei:
+        net.check()
+    assert ei.value.status == 2  # GPG_ERR_CUDA
+    assert torch.equal(got, ref)
+    net.set_wait_probe(0)
+    net.predict(rho, pin, got, float(CNST))
+    torch.cuda.synchronize()
+    net.check()
+    assert torch.equal(got, ref)
+    net.close()
