@@ -1,7 +1,7 @@
 """Time one configuration of the Poisson(-gravity) path on the device.
 
     python gpu_testbed_poisson-gravity_b200/run_config.py --scheme mg --ghost 3 --prec 4 \
-        --gra-ghost 2 --p5 --npatch 16384 [--gravity] [--reps 5] [--warm 3]
+        --gra-ghost 2 --p5 --npatch 16384 [--gravity] [--reps 5] [--warm 3] [--variant V]
 
 Seeded inputs from gpg.inputs (power-law density, analytic coarse potential,
 fluid when --gravity), reference parameters (gpg_default_params) unless
@@ -37,11 +37,17 @@ def main(argv=None) -> int:
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warm", type=int, default=3)
     ap.add_argument("--seed", type=int, default=21)
+    ap.add_argument("--variant", type=int, default=None, help="SOR kernel variant (gpg_set_sor_variant)")
     a = ap.parse_args(argv)
 
+    import ctypes as C
     import torch
-    from gpg.lib import solve_device
+    from gpg.lib import check, library, solve_device
     dev = torch.device("cuda:0")
+    if a.variant is not None:
+        check(library().gpg_set_sor_variant(a.prec, a.ghost, a.variant))
+        v = C.c_int()
+        check(library().gpg_get_sor_variant(a.prec, a.ghost, C.byref(v)))
     dt = np.float32 if a.prec == 4 else np.float64
     d = make_patches(a.npatch, a.ghost, seed=a.seed, gra_ghost=a.gra_ghost, dtype=dt, fluid=a.gravity)
     p = default_params(a.prec, a.ghost, GPG_SOR if a.scheme == "sor" else GPG_MG, gra_ghost=a.gra_ghost,
@@ -68,7 +74,7 @@ def main(argv=None) -> int:
     ms = s.elapsed_time(e) / max(1, a.reps)
     print(json.dumps({"scheme": a.scheme, "ghost": a.ghost, "prec": a.prec, "gra_ghost": a.gra_ghost, "p5": a.p5,
                       "gravity": a.gravity, "npatch": a.npatch, "ms": ms, "patches_per_s": a.npatch / ms * 1e3,
-                      "iters_mean": float(it.float().mean())}))
+                      "iters_mean": float(it.float().mean()), "variant": a.variant}))
     return 0
 
 
