@@ -21,7 +21,7 @@
 // Roles (17 warps):
 //   * producer warp (lane 0): streams the weights in 6 units per patch (up
 //     to 28 KB: 14 taps of a 32 -> 32 layer) through a 2-slot ring with TMA bulk
-//     copies (cp.async.bulk, no multicast), refilling a slot once the MMAs
+//     copies (cp.async.bulk into this CTA alone), refilling a slot once the MMAs
 //     that read it have completed (tcgen05.commit -> "empty" mbarrier).  The
 //     stream runs across layers and patches, so the next layer's weights land
 //     during the epilogue;

@@ -121,7 +121,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return mbar_wait_polls(bar, parity, err, 1u << 26);
 }
 
-// --- bulk copies (TMA, one-dimensional, no multicast) ----------------------
+// --- bulk copies (TMA, one-dimensional, into this CTA alone) --------------
 // The calling thread announces `bytes` of transaction on `bar` (one arrival);
 // each copy then completes its bytes on the barrier.  Source and destination
 // 16-byte aligned, sizes multiples of 16.
