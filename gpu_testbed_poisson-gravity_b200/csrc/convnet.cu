@@ -549,12 +549,14 @@ extern "C" int gpg_net_destroy(gpg_net *n) {
 
 extern "C" int gpg_net_get_params(gpg_net *n, float *host) {
   if (!n || !host) return nfail(GPG_ERR_INVALID, "NULL argument");
+  NET_CUDA(cudaSetDevice(n->device));
   NET_CUDA(cudaMemcpy(host, n->params, kParams * 4, cudaMemcpyDeviceToHost));
   return GPG_OK;
 }
 
 extern "C" int gpg_net_set_params(gpg_net *n, const float *host) {
   if (!n || !host) return nfail(GPG_ERR_INVALID, "NULL argument");
+  NET_CUDA(cudaSetDevice(n->device));
   NET_CUDA(cudaMemcpy(n->params, host, kParams * 4, cudaMemcpyHostToDevice));
   NET_CUDA(cudaMemset(n->adam_m, 0, kParams * 4));
   NET_CUDA(cudaMemset(n->adam_v, 0, kParams * 4));
@@ -564,6 +566,7 @@ extern "C" int gpg_net_set_params(gpg_net *n, const float *host) {
 
 extern "C" int gpg_net_check(gpg_net *n) {
   if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
+  NET_CUDA(cudaSetDevice(n->device));
   int flag = 0;
   NET_CUDA(cudaMemcpy(&flag, n->err, 4, cudaMemcpyDeviceToHost));
   if (flag) {
@@ -586,6 +589,7 @@ extern "C" int gpg_net_predict(gpg_net *n, int npatch, const float *d_rho, const
   if (npatch < 0) return nfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch && (!d_rho || !d_pot_in || !d_guess)) return nfail(GPG_ERR_INVALID, "NULL array");
   if (!npatch) return GPG_OK;
+  NET_CUDA(cudaSetDevice(n->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   static DevOnce once;
   using gpg::net::InferSmem;
@@ -613,6 +617,7 @@ extern "C" int gpg_net_predict_layers(gpg_net *n, int npatch, const float *d_rho
   if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
   if (npatch < 0) return nfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch && (!d_rho || !d_pot_in || !d_guess)) return nfail(GPG_ERR_INVALID, "NULL array");
+  NET_CUDA(cudaSetDevice(n->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   for (int64_t p0 = 0; p0 < npatch; p0 += n->max_batch) {
     const int64_t b = std::min<int64_t>(n->max_batch, npatch - p0);
@@ -628,6 +633,7 @@ extern "C" int gpg_net_gradients(gpg_net *n, int npatch, const float *d_rho, con
   if (!n) return nfail(GPG_ERR_INVALID, "net is NULL");
   if (npatch < 1 || npatch > n->max_batch) return nfail(GPG_ERR_INVALID, "npatch %d (1..%d)", npatch, n->max_batch);
   if (!d_rho || !d_pot_in || !d_target) return nfail(GPG_ERR_INVALID, "NULL array");
+  NET_CUDA(cudaSetDevice(n->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (int rc = gradients(n, npatch, d_rho, d_pot_in, d_target, float(cnst), d_loss, s)) return rc;
   if (d_grad) NET_CUDA(cudaMemcpyAsync(d_grad, n->grad, kParams * 4, cudaMemcpyDeviceToDevice, s));
@@ -655,5 +661,6 @@ extern "C" int gpg_net_train_step(gpg_net *n, int npatch, const float *d_rho, co
 
 extern "C" int gpg_net_apply_gradient(gpg_net *n, const float *d_grad, float lr, void *stream) {
   if (!n || !d_grad) return nfail(GPG_ERR_INVALID, "NULL argument");
+  NET_CUDA(cudaSetDevice(n->device));
   return adam_step(n, d_grad, lr, static_cast<cudaStream_t>(stream));
 }

@@ -279,6 +279,7 @@ extern "C" int gpg_lin_solve_device(gpg_lin *l, const gpg_params *p, int npatch,
   if (npatch < 0) return lfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch == 0) return GPG_OK;
   if (!d_rho || !d_pot_in || !d_pot_out || (p->gra_acc && !d_flu)) return lfail(GPG_ERR_INVALID, "NULL array");
+  LIN_CUDA(cudaSetDevice(l->device));
   // the inputs are staged with bulk copies of whole patches
   if ((reinterpret_cast<uintptr_t>(d_rho) | reinterpret_cast<uintptr_t>(d_pot_in)) & 15)
     return lfail(GPG_ERR_INVALID, "d_rho and d_pot_in must be 16-byte aligned");
@@ -311,6 +312,7 @@ extern "C" int gpg_lin_features(gpg_lin *l, const gpg_params *p, int npatch, con
   if (npatch < 0) return lfail(GPG_ERR_INVALID, "npatch %d", npatch);
   if (npatch == 0) return GPG_OK;
   if (!d_rho || !d_pot_in || !d_u || (d_target && !d_t)) return lfail(GPG_ERR_INVALID, "NULL array");
+  LIN_CUDA(cudaSetDevice(l->device));
   gpg_params q = *p;
   q.init_mode = GPG_INIT_INTERP;
   q.gra_acc = 0;
@@ -332,6 +334,7 @@ extern "C" int gpg_lin_gradients(gpg_lin *l, int npatch, const float *d_u, const
   if (!l) return lfail(GPG_ERR_INVALID, "lin is NULL");
   if (npatch < 1 || npatch > l->max_batch) return lfail(GPG_ERR_INVALID, "npatch %d (1..%d)", npatch, l->max_batch);
   if (!d_u || !d_t) return lfail(GPG_ERR_INVALID, "NULL array");
+  LIN_CUDA(cudaSetDevice(l->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   lin_err_kernel<<<npatch, 512, 0, s>>>(d_u, d_t, l->params, l->e, l->loss_part);
   lin_grad_kernel<<<64, 256, 0, s>>>(d_u, l->e, npatch, d_grad ? d_grad : l->grad);
@@ -359,6 +362,7 @@ extern "C" int gpg_lin_train_step(gpg_lin *l, int npatch, const float *d_u, cons
 
 extern "C" int gpg_lin_apply_gradient(gpg_lin *l, const float *d_grad, float lr, void *stream) {
   if (!l || !d_grad) return lfail(GPG_ERR_INVALID, "NULL argument");
+  LIN_CUDA(cudaSetDevice(l->device));
   return lin_adam(l, d_grad, lr, static_cast<cudaStream_t>(stream));
 }
 

@@ -290,6 +290,8 @@ GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
  * which 3 used, cout 16 for layer 4 of which 1 used).
  * ------------------------------------------------------------------------- */
 typedef struct gpg_net gpg_net;
+/* every call on a net makes the net's device current, as the gpg_context
+ * calls do; device arrays and streams passed to it belong to that device */
 GPG_API int gpg_net_create(gpg_net **net, int max_batch, uint64_t seed, int device_id);
 GPG_API int gpg_net_destroy(gpg_net *net);
 GPG_API int gpg_net_param_count(int64_t *count);
@@ -343,6 +345,7 @@ GPG_API const char *gpg_net_last_error(void);
  * persistent kernel; the correction never leaves the chip.
  * ------------------------------------------------------------------------- */
 typedef struct gpg_lin gpg_lin;
+/* every call on a lin makes its device current (as for gpg_net) */
 /* max_batch bounds npatch of gpg_lin_gradients / gpg_lin_train_step only;
  * parameters start at zero (delta = 0: the plain interpolated start) */
 GPG_API int gpg_lin_create(gpg_lin **lin, int max_batch, int device_id);
