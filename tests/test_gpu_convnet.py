@@ -1,8 +1,11 @@
 """Learned initial guess: tensor-core network vs its FP64 oracle (needs a B200).
 
 The oracle (oracle/convnet_oracle.py) rounds to bfloat16 where the kernels
-store bfloat16; what remains are FP32-vs-FP64 accumulation differences, so the
-checks are relative L2 errors (tolerances stated per test)."""
+store bfloat16; what remains are FP32-vs-FP64 accumulation differences (which
+now and then flip one bfloat16 rounding of an activation), so the checks are
+relative L2 errors.  Measured on B200 over four seeds: forward <= 6.3e-4,
+weight and bias gradients <= 2.3e-4, loss <= 1.6e-6; the tolerances below
+are 3-10x those."""
 import numpy as np
 import pytest
 
@@ -38,11 +41,12 @@ def rel(a, b):
     return float(np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
 
 
-def test_forward_matches_oracle(torch):
+@pytest.mark.parametrize("seed", [11, 33])
+def test_forward_matches_oracle(torch, seed):
     from gpg.net import Net, split_params
     from oracle.convnet_oracle import forward
-    rho, pin, _ = _data(3, 11)
-    net = Net(max_batch=4, seed=3)
+    rho, pin, _ = _data(3, seed)
+    net = Net(max_batch=4, seed=seed % 7 + 1)
     ws, bs = split_params(net.params().astype(np.float64))
     guess = torch.empty((3, 8, 8, 8), device="cuda")
     net.predict(torch.from_numpy(rho).cuda(), torch.from_numpy(pin).cuda(), guess, float(CNST))
@@ -51,15 +55,16 @@ def test_forward_matches_oracle(torch):
     x0, s = _oracle_inputs(rho, pin)
     _, y4 = forward(x0, ws, bs)
     want = y4[:, 1:-1, 1:-1, 1:-1, 0] * s[:, None, None, None]
-    assert rel(guess.cpu().numpy(), want) < 1e-2
+    assert rel(guess.cpu().numpy(), want) < 2e-3
     net.close()
 
 
-def test_gradients_match_oracle(torch):
+@pytest.mark.parametrize("seed", [21, 33])
+def test_gradients_match_oracle(torch, seed):
     from gpg.net import Net, split_params
     from oracle.convnet_oracle import loss_and_grads
-    rho, pin, tgt = _data(2, 21)
-    net = Net(max_batch=2, seed=5)
+    rho, pin, tgt = _data(3, seed)
+    net = Net(max_batch=4, seed=seed % 7 + 1)
     p = net.params()
     ws, bs = split_params(p.astype(np.float64))
     grad = torch.empty(net.nparams, device="cuda")
@@ -70,11 +75,11 @@ def test_gradients_match_oracle(torch):
     net.check()
     x0, s = _oracle_inputs(rho, pin)
     ol, odw, odb = loss_and_grads(x0, ws, bs, tgt, s)
-    assert abs(loss.item() - ol) <= 1e-3 * abs(ol)
+    assert abs(loss.item() - ol) <= 2e-5 * abs(ol)
     gws, gbs = split_params(grad.cpu().numpy().astype(np.float64))
     for l in range(4):
-        assert rel(gws[l], odw[l]) < 2e-2, (l, rel(gws[l], odw[l]))
-        assert rel(gbs[l], odb[l]) < 2e-2, (l, rel(gbs[l], odb[l]))
+        assert rel(gws[l], odw[l]) < 1e-3, (l, rel(gws[l], odw[l]))
+        assert rel(gbs[l], odb[l]) < 1e-3, (l, rel(gbs[l], odb[l]))
     net.close()
 
 

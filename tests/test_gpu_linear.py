@@ -13,8 +13,9 @@ the CPU restatement oracle/lin_oracle.py and the library's own plain SOR.
 import numpy as np
 import pytest
 
-from gpg.abi import (GPG_ERR_CUDA, GPG_INIT_INTERP, GPG_SOR, GPG_STOP_ABS_TOLERANCE, GPG_STOP_POT_TOLERANCE,
-                     GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE, default_params, fixed_residual_params)
+from gpg.abi import (GPG_ERR_CUDA, GPG_ERR_INVALID, GPG_INIT_INTERP, GPG_SOR, GPG_STOP_ABS_TOLERANCE,
+                     GPG_STOP_POT_TOLERANCE, GPG_STOP_REFERENCE, GPG_STOP_TOLERANCE, default_params,
+                     fixed_residual_params)
 from gpg.inputs import log_uniform, make_patches
 
 pytestmark = pytest.mark.gpu
@@ -308,7 +309,7 @@ def test_misaligned_inputs_are_rejected(torch, lin):
     rc = lib.gpg_lin_solve_device(lin._l, C.byref(p), 8, C.c_void_p(rho.data_ptr() + 4), C.c_void_p(pin.data_ptr()),
                                   C.c_void_p(out.data_ptr()), None, None, None,
                                   C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    assert rc == 1 and b"aligned" in lib.gpg_lin_last_error()
+    assert rc == GPG_ERR_INVALID and b"aligned" in lib.gpg_lin_last_error()
 
 
 def test_data_parallel_training_under_torchrun(torch, tmp_path):
