@@ -14,6 +14,16 @@
   with the macro set of Makefile:13-85; GPU_ARCH only has to name a known
   architecture for Header/Macro.h:27-31 and has no effect on CPU code.
 
+* ``build_ref_gpu()`` compiles the reference's GPU_API/ and GPU_Solver/
+  sources (the CUDA_FILE list of Makefile:164-167, read in place) for sm_100a
+  with nvcc, plus ``oracle/cuapi_bench.cpp``, into one timing executable per
+  configuration, ``oracle/_ref/cuapi_bench_ref_<cfg>``; ``build_cuapi_bench()``
+  links the same driver on this library's CUAPI shim and libgpg
+  (``oracle/_ref/cuapi_bench_gpg_<cfg>``), so both run the same calls on the
+  same inputs.  The nvcc flags follow Makefile:195-206 (-O3, -Xptxas -dlcm=ca
+  for the CUPOT files) with the reference's macro set; ``ref_gpu_compat.h`` is
+  force-included for the one pre-Volta intrinsic.
+
 Run ``python oracle/build.py [--ref /path/to/reference]``.
 """
 from __future__ import annotations
@@ -163,6 +173,96 @@ def build_ref(ref_root: str = DEFAULT_REF, jobs: int | None = None) -> list[str]
         return [f.result() for f in futs]
 
 
+# ---------------------------------------------------------------------------
+# the reference's own GPU path recompiled for sm_100a, and the same timing
+# driver on this library (test infrastructure: tests/test_gpu_reference_gpu.py)
+# ---------------------------------------------------------------------------
+REF_GPU_API = ["CUAPI_Set_Diagnose_Device.cu", "CUAPI_Synchronize.cu", "CUAPI_Asyn_PoissonGravitySolver.cu",
+               "CUAPI_MemAllocate_PoissonGravity.cu", "CUAPI_MemFree_PoissonGravity.cu"]
+REF_GPU_SOLVER = ["CUPOT_PoissonSolver_SOR_10to14cube.cu", "CUPOT_PoissonSolver_SOR_16to18cube.cu",
+                  "CUPOT_GravitySolver.cu", "CUPOT_PoissonSolver_MG.cu"]
+BENCH_DRIVER = os.path.join(HERE, "cuapi_bench.cpp")
+GPU_COMPAT = os.path.join(HERE, "ref_gpu_compat.h")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
+# (scheme, POT_GHOST_SIZE, GRA_GHOST_SIZE, precision): SOR at every ghost size
+# and precision, MG in FP32 up to ghost 4 (its FP64 and 18^3 forms take
+# per-block device malloc, CUPOT_PoissonSolver_MG.cu:136-145,186-187, which
+# these comparisons leave out)
+REF_GPU_CONFIGS = ([("sor", g, 1, p) for g in range(1, 6) for p in ("f32", "f64")]
+                   + [("sor", 3, 2, "f32"), ("mg", 3, 2, "f32")])
+
+
+def cuapi_bench_exe(kind: str, scheme: str, g: int, G: int, prec: str) -> str:
+    return os.path.join(REF_OUT, f"cuapi_bench_{kind}_{scheme}_g{g}_G{G}_{prec}")
+
+
+def _bench_macros(scheme, g, G, prec):
+    poi, gra = MAXERR[(scheme, prec)]
+    return reference_macros(scheme, g, G, prec) + [
+        "-DCPULOAD=420000", "-DINIT_WIDTH=410.0", "-DINIT_INDEX=2.1", "-DINIT_OFFSET=0.09",
+        f"-DPOI_MAXERR={poi}", f"-DGRA_MAXERR={gra}"]
+
+
+def _build_ref_gpu_one(ref_root, scheme, g, G, prec):
+    out = cuapi_bench_exe("ref", scheme, g, G, prec)
+    cus = ([os.path.join(ref_root, "GPU_API", f) for f in REF_GPU_API]
+           + [os.path.join(ref_root, "GPU_Solver", f) for f in REF_GPU_SOLVER])
+    hdrs = [os.path.join(ref_root, "Header", h) for h in os.listdir(os.path.join(ref_root, "Header"))]
+    incl = [os.path.join(ref_root, "GPU_Solver", f) for f in os.listdir(os.path.join(ref_root, "GPU_Solver"))]
+    aux = [os.path.join(ref_root, s) for s in REF_SOURCES if s.startswith("Auxiliary/")]
+    deps = cus + hdrs + incl + aux + [BENCH_DRIVER, GPU_COMPAT]
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+        return out
+    macros = _bench_macros(scheme, g, G, prec)
+    inc = ["-I" + os.path.join(ref_root, "Header"), "-I" + os.path.join(ref_root, "GPU_Solver")]
+    objs = []
+    for src in cus:
+        obj = out + "_" + os.path.basename(src).replace(".cu", ".o")
+        extra = ["-Xptxas", "-dlcm=ca"] if os.path.basename(src).startswith("CUPOT_") else []
+        _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-w", "-include", GPU_COMPAT]
+             + extra + inc + macros + ["-c", "-o", obj, src])
+        objs.append(obj)
+    _run(["g++", "-O3", "-w", "-DREF_GPU", "-I" + os.path.join(CUDA_LIB, "..", "include")] + inc + macros
+         + ["-o", out, BENCH_DRIVER] + aux + objs + ["-L" + CUDA_LIB, "-lcudart", "-Wl,-rpath," + CUDA_LIB])
+    for o in objs:
+        os.remove(o)
+    return out
+
+
+def _build_cuapi_bench_one(ref_root, scheme, g, G, prec):
+    out = cuapi_bench_exe("gpg", scheme, g, G, prec)
+    aux = [os.path.join(ref_root, s) for s in REF_SOURCES if s.startswith("Auxiliary/")]
+    deps = aux + [BENCH_DRIVER, SHIM, os.path.join(REPO, "include", "gpg_cuapi.h"),
+                  os.path.join(LIBGPG_DIR, "libgpg.so")]
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+        return out
+    macros = _bench_macros(scheme, g, G, prec)
+    shim_macros = [m for m in macros if not m.startswith("-DPOT_SCHEME")] + [
+        f"-DPOT_SCHEME={1 if scheme == 'sor' else 2}"]
+    shim_obj = out + "_shim.o"
+    _run(["g++", "-O2", "-fPIC", "-c", "-o", shim_obj, SHIM] + shim_macros)
+    _run(["g++", "-O3", "-w", "-I" + os.path.join(ref_root, "Header")] + macros
+         + ["-o", out, BENCH_DRIVER] + aux + [shim_obj, "-L" + LIBGPG_DIR, "-lgpg",
+                                              "-Wl,-rpath,$ORIGIN/../../gpu_testbed_poisson-gravity_b200/lib"])
+    os.remove(shim_obj)
+    return out
+
+
+def build_ref_gpu(ref_root: str = DEFAULT_REF) -> list[str]:
+    """Both timing executables of every REF_GPU_CONFIGS entry (reference GPU
+    path for sm_100a; this library through its CUAPI shim)."""
+    if not os.path.isdir(os.path.join(ref_root, "GPU_Solver")):
+        return []
+    if not os.path.exists(os.path.join(LIBGPG_DIR, "libgpg.so")):
+        raise RuntimeError("build libgpg.so first")
+    os.makedirs(REF_OUT, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        futs = [ex.submit(_build_ref_gpu_one, ref_root, *c) for c in REF_GPU_CONFIGS]
+        futs += [ex.submit(_build_cuapi_bench_one, ref_root, *c) for c in REF_GPU_CONFIGS]
+        return [f.result() for f in futs]
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--ref", default=DEFAULT_REF)
@@ -174,6 +274,8 @@ def main(argv=None) -> int:
         print(f"{len(libs)} reference configurations in {REF_OUT}")
         exes = build_integration(a.ref)
         print(f"{len(exes)} integration executables in {REF_OUT}")
+        exes = build_ref_gpu(a.ref)
+        print(f"{len(exes)} CUAPI timing executables in {REF_OUT}")
     return 0
 
 
