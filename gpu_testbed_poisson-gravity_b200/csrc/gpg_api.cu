@@ -499,8 +499,6 @@ struct gpg_context {
   int32_t *d_iters = nullptr;
   double *d_resid = nullptr;
   void *h_rho = nullptr, *h_pin = nullptr, *h_pout = nullptr, *h_flu = nullptr;
-  int32_t *h_iters = nullptr;
-  double *h_resid = nullptr;
   int64_t last_npatch = 0;
 };
 
@@ -551,13 +549,9 @@ static void release_buffers(gpg_context *c) {
   cudaFree(c->d_flu);
   cudaFree(c->d_iters);
   cudaFree(c->d_resid);
-  cudaFreeHost(c->h_iters);
-  cudaFreeHost(c->h_resid);
   c->d_rho = c->d_pin = c->d_pout = c->d_flu = nullptr;
   c->d_iters = nullptr;
   c->d_resid = nullptr;
-  c->h_iters = nullptr;
-  c->h_resid = nullptr;
   c->cap = 0;
   c->allocated = false;
   c->last_npatch = 0;  // gpg_last_iterations has nothing to read any more
@@ -587,8 +581,6 @@ extern "C" int gpg_mem_allocate(gpg_context *ctx, const gpg_params *shape, int n
   if (int rc = chk(cudaMalloc(&ctx->d_flu, b_flu), "cudaMalloc flu")) return rc;
   if (int rc = chk(cudaMalloc(&ctx->d_iters, sizeof(int32_t) * (n ? n : 1)), "cudaMalloc iters")) return rc;
   if (int rc = chk(cudaMalloc(&ctx->d_resid, sizeof(double) * (n ? n : 1)), "cudaMalloc resid")) return rc;
-  if (int rc = chk(cudaMallocHost(&ctx->h_iters, sizeof(int32_t) * (n ? n : 1)), "cudaMallocHost iters")) return rc;
-  if (int rc = chk(cudaMallocHost(&ctx->h_resid, sizeof(double) * (n ? n : 1)), "cudaMallocHost resid")) return rc;
   // pinned host arrays handed to the caller (CUAPI_MemAllocate_PoissonGravity.cu:66-69)
   void **outs[4] = {h_rho, h_pot_in, h_pot_out, h_flu};
   const size_t sizes[4] = {b_rho, b_pin, b_pout, b_flu};
@@ -705,8 +697,6 @@ extern "C" int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_r
     if (p->poisson) {
       GPG_CUDA(cudaMemcpyAsync(bp(h_pot_out, f * ctx->n_pout * es), bp(ctx->d_pout, f * ctx->n_pout * es),
                                c * ctx->n_pout * es, cudaMemcpyDeviceToHost, st));
-      GPG_CUDA(cudaMemcpyAsync(ctx->h_iters + f, ctx->d_iters + f, c * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-      GPG_CUDA(cudaMemcpyAsync(ctx->h_resid + f, ctx->d_resid + f, c * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     if (p->gra_acc)
       GPG_CUDA(cudaMemcpyAsync(bp(h_flu, f * ctx->n_flu * es), bp(ctx->d_flu, f * ctx->n_flu * es),
@@ -730,8 +720,13 @@ extern "C" int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *res
   if (!ctx) return fail(GPG_ERR_INVALID, "context is NULL");
   if (npatch < 0 || npatch > ctx->last_npatch)
     return fail(GPG_ERR_INVALID, "npatch %d (last solve had %lld)", npatch, (long long)ctx->last_npatch);
-  if (iters && npatch) std::memcpy(iters, ctx->h_iters, sizeof(int32_t) * npatch);
-  if (resid && npatch) std::memcpy(resid, ctx->h_resid, sizeof(double) * npatch);
+  // read from the device on request: the per-call solve moves no per-patch
+  // diagnostics over the host link
+  GPG_CUDA(cudaSetDevice(ctx->device));
+  for (auto s : ctx->streams) GPG_CUDA(cudaStreamSynchronize(s));
+  if (iters && npatch)
+    GPG_CUDA(cudaMemcpy(iters, ctx->d_iters, sizeof(int32_t) * npatch, cudaMemcpyDeviceToHost));
+  if (resid && npatch) GPG_CUDA(cudaMemcpy(resid, ctx->d_resid, sizeof(double) * npatch, cudaMemcpyDeviceToHost));
   return GPG_OK;
 }
 

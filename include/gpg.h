@@ -175,9 +175,10 @@ GPG_API int gpg_asyn_poisson_gravity_solver(gpg_context *ctx, const void *h_rho,
 /* CUAPI_Synchronize (GPU_API/CUAPI_Synchronize.cu:10-13). */
 GPG_API int gpg_synchronize(gpg_context *ctx);
 
-/* Per-patch iteration counts / residuals of the last completed solve (host
- * copies; valid after gpg_synchronize).  No reference counterpart: the
- * reference only prints them (CPU_PoissonSolver_SOR.cpp:288). */
+/* Per-patch iteration counts / residuals of the last solve, read from the
+ * device on request (the call waits for the context's streams).  No
+ * reference counterpart: the reference only prints them
+ * (CPU_PoissonSolver_SOR.cpp:288). */
 GPG_API int gpg_last_iterations(gpg_context *ctx, int32_t *iters, double *resid, int npatch);
 
 /* ---------------------------------------------------------------------------
