@@ -53,14 +53,18 @@ def test_reference_gpu_path_agrees_on_b200(case, tmp_path):
     write_inputs(case, fin)
     res = {}
     outs = {}
-    for kind, exe in (("reference_gpu_sm100a", exe_ref), ("this_library", exe_gpg)):
-        fout = str(tmp_path / f"out_{kind}.bin")
-        r = subprocess.run([exe] + driver_args(case, fin, fout), capture_output=True, text=True, timeout=600)
-        assert r.returncode == 0, (kind, r.stdout[-2000:], r.stderr[-2000:])
-        res[kind] = json.loads(r.stdout.strip().splitlines()[-1])
-        raw = np.fromfile(fout, dtype=dt)
-        gn = 8 + 2 * G
-        outs[kind] = (raw[:npatch * gn ** 3], raw[npatch * gn ** 3:])
+    try:
+        for kind, exe in (("reference_gpu_sm100a", exe_ref), ("this_library", exe_gpg)):
+            fout = str(tmp_path / f"out_{kind}.bin")
+            r = subprocess.run([exe] + driver_args(case, fin, fout), capture_output=True, text=True, timeout=600)
+            assert r.returncode == 0, (kind, r.stdout[-2000:], r.stderr[-2000:])
+            res[kind] = json.loads(r.stdout.strip().splitlines()[-1])
+            raw = np.fromfile(fout, dtype=dt)
+            os.remove(fout)
+            gn = 8 + 2 * G
+            outs[kind] = (raw[:npatch * gn ** 3], raw[npatch * gn ** 3:])
+    finally:
+        os.remove(fin)  # up to 275 MB per case
     poi, gra = (float(x) for x in ob.MAXERR[(scheme, prec)])
     mine, ref = outs["this_library"], outs["reference_gpu_sm100a"]
     pot_err = _scaled(mine[0].reshape(npatch, 1, -1), ref[0].reshape(npatch, 1, -1))
