@@ -27,15 +27,20 @@ from gpg.inputs import make_patches  # noqa: E402
 
 from oracle.build import REF_GPU_CONFIGS  # noqa: E402
 
-# (scheme, ghost, GRA ghost, precision) -> patches, P5 gradient: SOR on the
+# (scheme, ghost, GRA ghost, precision, patches, P5 gradient): SOR on the
 # 4096-patch batches of the plain-SOR workload, MG on 16384 patches with the
-# 5-point gradient
-CASES = {c: (16384 if c[0] == "mg" else 4096, 1 if c[0] == "mg" else 0) for c in REF_GPU_CONFIGS}
+# 5-point gradient, and the reference README's own GPU benchmark sizes
+# (README.txt:114-150: 256 patches at ghost 1 and 3)
+CASES = ([c + ((16384, 1) if c[0] == "mg" else (4096, 0)) for c in REF_GPU_CONFIGS]
+         + [("sor", 1, 1, "f32", 256, 0), ("sor", 3, 1, "f32", 256, 0)])
+
+
+def case_id(case) -> str:
+    return "{}_g{}_G{}_{}_{}".format(*case[:5])
 
 
 def write_inputs(case, path: str) -> None:
-    scheme, g, G, prec = case
-    npatch, _ = CASES[case]
+    scheme, g, G, prec, npatch, _ = case
     dt = np.float64 if prec == "f64" else np.float32
     d = make_patches(npatch, g, seed=61 + g, gra_ghost=G, dtype=dt, fluid=True)
     with open(path, "wb") as f:
@@ -44,8 +49,7 @@ def write_inputs(case, path: str) -> None:
 
 
 def driver_args(case, fin: str, fout: str, reps: int = 10, warm: int = 2) -> list[str]:
-    scheme, g, G, prec = case
-    npatch, p5 = CASES[case]
+    scheme, g, G, prec, npatch, p5 = case
     f64 = prec == "f64"
     return ["--in", fin, "--out", fout, "--npg", str(npatch // 8), "--nstream", "4", "--reps", str(reps),
             "--warm", str(warm), "--min-iter", "10", "--max-iter", "100" if f64 else "60",
@@ -60,13 +64,16 @@ def main(argv=None) -> int:
     ap.add_argument("gra_ghost", type=int)
     ap.add_argument("prec", choices=["f32", "f64"])
     ap.add_argument("input_file")
+    ap.add_argument("--npatch", type=int, default=None, help="patches (default: the case's first size)")
     ap.add_argument("--out", default=os.devnull)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--warm", type=int, default=2)
     a = ap.parse_args(argv)
-    case = (a.scheme, a.ghost, a.gra_ghost, a.prec)
-    if case not in CASES:
-        ap.error(f"no such case; built cases: {sorted(CASES)}")
+    found = [c for c in CASES if c[:4] == (a.scheme, a.ghost, a.gra_ghost, a.prec)
+             and (a.npatch is None or c[4] == a.npatch)]
+    if not found:
+        ap.error(f"no such case; cases: {[case_id(c) for c in CASES]}")
+    case = found[0]
     write_inputs(case, a.input_file)
     print(" ".join(driver_args(case, a.input_file, a.out, a.reps, a.warm)))
     return 0

@@ -29,7 +29,7 @@ import numpy as np
 import pytest
 
 from oracle import build as ob
-from oracle.cuapi_bench_inputs import CASES, driver_args, write_inputs
+from oracle.cuapi_bench_inputs import CASES, case_id, driver_args, write_inputs
 
 pytestmark = pytest.mark.gpu
 
@@ -41,13 +41,12 @@ def _scaled(a, b):
     return np.abs(b - a) / np.abs(a).max(axis=2, keepdims=True)
 
 
-@pytest.mark.parametrize("case", list(CASES), ids=lambda c: "{}_g{}_G{}_{}".format(*c))
+@pytest.mark.parametrize("case", CASES, ids=case_id)
 def test_reference_gpu_path_agrees_on_b200(case, tmp_path):
-    scheme, g, G, prec = case
-    exe_ref, exe_gpg = ob.cuapi_bench_exe("ref", *case), ob.cuapi_bench_exe("gpg", *case)
+    scheme, g, G, prec, npatch, p5 = case
+    exe_ref, exe_gpg = ob.cuapi_bench_exe("ref", *case[:4]), ob.cuapi_bench_exe("gpg", *case[:4])
     if not (os.path.exists(exe_ref) and os.path.exists(exe_gpg)):
         pytest.skip("reference GPU build absent (oracle/build.py build_ref_gpu needs the reference tree)")
-    npatch, p5 = CASES[case]
     dt = np.float64 if prec == "f64" else np.float32
     fin = str(tmp_path / "in.bin")
     write_inputs(case, fin)
@@ -69,7 +68,7 @@ def test_reference_gpu_path_agrees_on_b200(case, tmp_path):
     mine, ref = outs["this_library"], outs["reference_gpu_sm100a"]
     pot_err = _scaled(mine[0].reshape(npatch, 1, -1), ref[0].reshape(npatch, 1, -1))
     flu_err = _scaled(mine[1].reshape(npatch, 5, -1), ref[1].reshape(npatch, 5, -1))
-    line = {"case": "{}_g{}_G{}_{}".format(*case), "npatch": npatch, "p5": p5,
+    line = {"case": case_id(case), "npatch": npatch, "p5": p5,
             "pot_err_max": float(pot_err.max()), "pot_err_p999": float(np.percentile(pot_err, 99.9)),
             "pot_patches_differing": int((pot_err.reshape(npatch, -1).max(1) > 0).sum()),
             "flu_err_max": float(flu_err.max()), **res}

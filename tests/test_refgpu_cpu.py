@@ -8,17 +8,17 @@ import pytest
 
 from gpg.abi import SOR_OMEGA
 from oracle import build as ob
-from oracle.cuapi_bench_inputs import CASES, driver_args
+from oracle.cuapi_bench_inputs import CASES, case_id, driver_args
 
 
 def _kv(args):
     return dict(zip(args[::2], args[1::2]))
 
 
-@pytest.mark.parametrize("case", list(CASES), ids=lambda c: "{}_g{}_G{}_{}".format(*c))
+@pytest.mark.parametrize("case", CASES, ids=case_id)
 def test_driver_arguments_follow_the_reference_defaults(case):
-    scheme, g, G, prec = case
-    npatch, p5 = CASES[case]
+    scheme, g, G, prec, npatch, p5 = case
+    assert case[:4] in ob.REF_GPU_CONFIGS
     a = _kv(driver_args(case, "in.bin", "out.bin"))
     assert int(a["--npg"]) * 8 == npatch
     assert a["--max-iter"] == ("100" if prec == "f64" else "60") and a["--min-iter"] == "10"
