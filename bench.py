@@ -874,6 +874,11 @@ def main(argv=None) -> int:
 
     wavefronts = wavefronts_of(pk, iters[k])
     vk, zk, yk, acck = layout(pk)
+    import ctypes as C
+    from gpg.lib import check
+    stg = C.c_int()
+    check(library().gpg_sor_variant_staged(vk, C.byref(stg)))
+    kname = "staged_sor_kernel" if stg.value else "sor_kernel"
     onchip = {"resource": "shared-memory pipe", "unit": "wavefronts/s",
               "achieved": wavefronts / (launch_ms / 1e3), "peak": onchip_peak,
               "frac": wavefronts / (launch_ms / 1e3) / onchip_peak,
@@ -903,7 +908,7 @@ def main(argv=None) -> int:
             f"f{8 * p.real_size}_g{p.ghost}":
                 wavefronts_of(p, it) / (float(per_kernel[:, i].mean()) / 1e3) / onchip_peak
             for i, ((p, _), it) in enumerate(zip(batches, iters))},
-        "roofline": {"bound": "hbm", "kernel": f"sor_kernel f{8 * pk.real_size} g{pk.ghost}",
+        "roofline": {"bound": "hbm", "kernel": f"{kname} f{8 * pk.real_size} g{pk.ghost}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
                      "launch_ms": launch_ms, "peak_source": "measured" if peaks else "fallback",

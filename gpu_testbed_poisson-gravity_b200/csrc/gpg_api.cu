@@ -11,6 +11,8 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
+#include <limits>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -112,10 +114,33 @@ constexpr int kSorVariantRows[kSorVariants] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 
 constexpr bool kSorVariantStaged[kSorVariants] = {false, false, false, false, false, false, false, false, false,
                                                   false, false, false, false, false, true,  true,  true};
 // atomic: gpg_set_sor_variant may run on one host thread while another launches
+constexpr int kSorDefault[2][6] = {
+    // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters;
+    //                                  FP32 g4 / g5 and FP64 g5 confirmed by three A/B bench runs)
+    {0, 10, 11, 10, 10, 15},   // float
+    {0, 11, 13, 11, 10, 14},   // double
+};
 std::atomic<int> g_sor_variant[2][6] = {
-    // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters)
-    {0, 10, 11, 10, 11, 10},   // float
-    {0, 11, 13, 11, 10, 11},   // double
+    {kSorDefault[0][0], kSorDefault[0][1], kSorDefault[0][2], kSorDefault[0][3], kSorDefault[0][4], kSorDefault[0][5]},
+    {kSorDefault[1][0], kSorDefault[1][1], kSorDefault[1][2], kSorDefault[1][3], kSorDefault[1][4], kSorDefault[1][5]},
+};
+// set once a variant was chosen explicitly (gpg_set_sor_variant or the tuning
+// file): every launch then uses it, whatever its size
+std::atomic<bool> g_sor_pinned[2][6] = {};
+// Small launches: at a few thousand patches and fewer a launch leaves SMs
+// short of teams, and the layouts that split each pair column between two
+// lanes (twice the threads per patch) finish each patch sooner.  Measured on
+// B200 at 64-4096 patches per launch (reference parameters, gravity on), the
+// variant below wins up to max_npatch patches: FP32 ghost 1 at 256 patches
+// 18.7 -> 13.2 us per launch, ghost 2 18.7 -> 12.5, ghost 5 at 2048 166 -> 145;
+// FP64 ghost 2 at 256 53.5 -> 39.1.  Beyond it the table above holds.
+struct SorSmall {
+  int max_npatch, variant;
+};
+constexpr SorSmall kSorSmall[2][6] = {
+    // ghost:  -       1          2          3         4           5
+    {{0, 0}, {2048, 6}, {2048, 6}, {2048, 7}, {256, 7}, {2048, 11}},   // float
+    {{0, 0}, {256, 8}, {256, 7}, {0, 0}, {0, 0}, {0, 0}},              // double
 };
 std::once_flag g_tune_once;
 
@@ -140,8 +165,10 @@ void load_tune_file() {
   int g, v;
   while (std::fscanf(f, "%7s %d %d", prec, &g, &v) == 3) {
     const int t = std::strcmp(prec, "f64") == 0 ? 1 : (std::strcmp(prec, "f32") == 0 ? 0 : -1);
-    if (t >= 0 && g >= 1 && g <= 5 && v >= 0 && v < kSorVariants)
+    if (t >= 0 && g >= 1 && g <= 5 && v >= 0 && v < kSorVariants) {
       g_sor_variant[t][g].store(v, std::memory_order_relaxed);
+      g_sor_pinned[t][g].store(true, std::memory_order_relaxed);
+    }
   }
   std::fclose(f);
 }
@@ -242,10 +269,28 @@ int prepare_staged_v() {
   }
 }
 
+// Set on the host thread that prepares and captures a concurrent batch plan:
+// its branches share the SMs, and a staged persistent kernel, whose CTAs take
+// patches at a fixed stride, then finishes with a tail (65,536 mixed patches:
+// 1.43 vs 1.34 ms per graph launch), so staged variants run as their unstaged layouts there.
+thread_local bool t_shared_sms = false;
+struct SharedSms {
+  SharedSms() { t_shared_sms = true; }
+  ~SharedSms() { t_shared_sms = false; }
+};
+
+// the variant a launch of npatch patches runs
+inline int sor_variant_for(bool f64, int g, int64_t npatch) {
+  int v = g_sor_variant[f64][g].load(std::memory_order_relaxed);
+  const SorSmall &sm = kSorSmall[f64][g];
+  if (!g_sor_pinned[f64][g].load(std::memory_order_relaxed) && npatch <= sm.max_npatch) v = sm.variant;
+  if (t_shared_sms && kSorVariantStaged[v]) v = v == 14 ? 10 : (v == 15 ? 11 : 13);  // same layout, unstaged
+  return v;
+}
+
 template <typename T, int G>
-int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
-  std::call_once(g_tune_once, load_tune_file);
-  switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
+int launch_sor_variant(int variant, const gpg::SolveArgs<T> &a, cudaStream_t s) {
+  switch (variant) {
     case 0: return launch_sor_v<T, G, 1, false, 1, 1>(a, s);
     case 1: return launch_sor_v<T, G, 1, true, 1, 1>(a, s);
     case 2: return launch_sor_v<T, G, 2, false, 1, 1>(a, s);
@@ -267,9 +312,14 @@ int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
 }
 
 template <typename T, int G>
-int prepare_sor() {
+int launch_sor(const gpg::SolveArgs<T> &a, cudaStream_t s) {
   std::call_once(g_tune_once, load_tune_file);
-  switch (g_sor_variant[sizeof(T) == 8][G].load(std::memory_order_relaxed)) {
+  return launch_sor_variant<T, G>(sor_variant_for(sizeof(T) == 8, G, a.npatch), a, s);
+}
+
+template <typename T, int G>
+int prepare_sor_variant(int variant) {
+  switch (variant) {
     case 0: return prepare_sor_v<T, G, 1, false, 1, 1>();
     case 1: return prepare_sor_v<T, G, 1, true, 1, 1>();
     case 2: return prepare_sor_v<T, G, 2, false, 1, 1>();
@@ -288,6 +338,16 @@ int prepare_sor() {
     case 15: return prepare_staged_v<T, G, true, 2, 2>();
     default: return prepare_staged_v<T, G, true, 1, 2>();
   }
+}
+
+// attributes of both variants a launch may pick (large and small batches)
+template <typename T, int G>
+int prepare_sor() {
+  std::call_once(g_tune_once, load_tune_file);
+  constexpr bool f64 = sizeof(T) == 8;
+  const int large = sor_variant_for(f64, G, std::numeric_limits<int64_t>::max()), small = sor_variant_for(f64, G, 0);
+  if (int rc = prepare_sor_variant<T, G>(large)) return rc;
+  return small == large ? GPG_OK : prepare_sor_variant<T, G>(small);
 }
 
 template <typename T>
@@ -797,9 +857,12 @@ extern "C" int gpg_sor_layout(int real_size, int ghost, int variant, int *fields
 
 extern "C" int gpg_set_sor_variant(int real_size, int ghost, int variant) {
   std::call_once(g_tune_once, load_tune_file);
-  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < 0 || variant >= kSorVariants)
+  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || variant < -1 || variant >= kSorVariants)
     return fail(GPG_ERR_INVALID, "real_size %d ghost %d variant %d", real_size, ghost, variant);
-  g_sor_variant[real_size == 8][ghost].store(variant, std::memory_order_relaxed);
+  const int t = real_size == 8;
+  // -1: back to the library's own choice (built-in table and small-batch rule)
+  g_sor_variant[t][ghost].store(variant < 0 ? kSorDefault[t][ghost] : variant, std::memory_order_relaxed);
+  g_sor_pinned[t][ghost].store(variant >= 0, std::memory_order_relaxed);
   return GPG_OK;
 }
 
@@ -975,6 +1038,7 @@ extern "C" int gpg_batch_plan_create(gpg_batch_plan **out, const gpg_params *p, 
   if (mode != GPG_PLAN_PERSISTENT && mode != GPG_PLAN_CONCURRENT) return fail(GPG_ERR_INVALID, "mode %d", mode);
   if (int rc = validate_batch(p, ngroup, groups)) return rc;
   GPG_CUDA(cudaSetDevice(device_id));
+  std::unique_ptr<SharedSms> shared(mode == GPG_PLAN_CONCURRENT ? new SharedSms : nullptr);
   if (mode == GPG_PLAN_CONCURRENT) {
     // every kernel the branches launch gets its attributes outside the capture
     for (int i = 0; i < ngroup; ++i) {

@@ -261,7 +261,11 @@ GPG_API int gpg_batch_plan_destroy(gpg_batch_plan *plan);
  * Variants 0-5 return identical bits; the others sum the residual in another
  * order, so a stop decision can differ only where two sweeps' totals tie.  The table starts from the library's defaults, then an optional
  * tuning file ($GPG_TUNE_FILE, else sor_tune.txt beside libgpg.so, lines
- * "f32|f64 <ghost> <variant>") written by autotune.py.
+ * "f32|f64 <ghost> <variant>") written by autotune.py.  Unless a variant was
+ * chosen (by gpg_set_sor_variant or the tuning file), launches of up to a
+ * stated number of patches (256 or 2048, per precision and ghost size) run a
+ * small-batch variant instead, one that gives each patch more threads;
+ * gpg_get_sor_variant reports the large-batch choice.
  * ------------------------------------------------------------------------- */
 GPG_API int gpg_sor_variant_count(void);
 GPG_API int gpg_sor_variant_info(int variant, int *patches_per_cta, int *phased);
@@ -277,6 +281,7 @@ GPG_API int gpg_sor_variant_staged(int variant, int *staged);
  * (c * (8 + 2 ghost) + z) * PP + y * P + (x + 1) / 2. */
 #define GPG_SOR_LAYOUT_FIELDS 11
 GPG_API int gpg_sor_layout(int real_size, int ghost, int variant, int *fields);
+/* variant -1 returns (real_size, ghost) to the library's built-in choice */
 GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
 GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
 

@@ -97,3 +97,13 @@ def test_sor_variant_table_queries():
             check(lib.gpg_sor_variant_layout(bad, None, None))
     with pytest.raises(GpgError):
         check(lib.gpg_set_sor_variant(4, 3, n))
+    with pytest.raises(GpgError):
+        check(lib.gpg_set_sor_variant(4, 3, -2))
+    # -1 hands the choice back to the library: its built-in large-batch variant
+    before = C.c_int()
+    check(lib.gpg_get_sor_variant(4, 3, C.byref(before)))
+    check(lib.gpg_set_sor_variant(4, 3, (before.value + 1) % n))
+    check(lib.gpg_set_sor_variant(4, 3, -1))
+    after = C.c_int()
+    check(lib.gpg_get_sor_variant(4, 3, C.byref(after)))
+    assert after.value == before.value
