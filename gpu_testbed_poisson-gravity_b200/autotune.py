@@ -7,6 +7,10 @@ bits, and writes the fastest choice to lib/sor_tune.txt beside libgpg.so,
 which the library reads on first use (include/gpg.h, gpg_set_sor_variant).
 
     python gpu_testbed_poisson-gravity_b200/autotune.py [--npatch 4096] [--json out.json]
+
+With --sizes (a comma-separated list of patch counts) it only reports: every
+variant's time at each size, for choosing the small-launch table (kSorSmall
+in csrc/gpg_api.cu); --gravity adds the fused gravity update to each launch.
 """
 from __future__ import annotations
 
@@ -39,13 +43,14 @@ def variants():
 
 
 def time_variant(torch, p, t, reps=5, warm=2):
+    flu = t.get("flu")
     for _ in range(warm):
-        solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], iters=t["iters"], resid=t["resid"])
+        solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], flu=flu, iters=t["iters"], resid=t["resid"])
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
     for _ in range(reps):
-        solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], iters=t["iters"], resid=t["resid"])
+        solve_device(p, t["rho"], t["pot_in"], pot_out=t["pot_out"], flu=flu, iters=t["iters"], resid=t["resid"])
     e.record()
     torch.cuda.synchronize()
     return s.elapsed_time(e) / reps
@@ -94,12 +99,55 @@ def tune(npatch=4096, precisions=(4, 8), ghosts=(1, 2, 3, 4, 5)):
     return report
 
 
+def sizes_report(sizes, gravity: bool, precisions=(4, 8), ghosts=(1, 2, 3, 4, 5), reps=50):
+    """Every variant's launch time (microseconds, CUDA events, mean of reps
+    after 5 warm-up launches) at each patch count; the library's own choice
+    is restored afterwards (gpg_set_sor_variant -1)."""
+    import torch
+    lib = library()
+    dev = torch.device("cuda:0")
+    out = []
+    for rs in precisions:
+        for g in ghosts:
+            for n in sizes:
+                dt = np.float32 if rs == 4 else np.float64
+                d = make_patches(n, g, seed=21, dtype=dt, fluid=gravity)
+                tdt = torch.float32 if rs == 4 else torch.float64
+                t = dict(rho=torch.from_numpy(d["rho"]).to(dev), pot_in=torch.from_numpy(d["pot_in"]).to(dev),
+                         pot_out=torch.empty((n, 10, 10, 10), dtype=tdt, device=dev),
+                         iters=torch.empty(n, dtype=torch.int32, device=dev),
+                         resid=torch.empty(n, dtype=torch.float64, device=dev))
+                if gravity:
+                    t["flu"] = torch.from_numpy(d["flu"]).to(dev)
+                p = default_params(rs, g, GPG_SOR, gra_acc=int(gravity))
+                row = {}
+                for v, *_ in variants():
+                    check(lib.gpg_set_sor_variant(rs, g, v))
+                    try:
+                        row[v] = round(1e3 * time_variant(torch, p, t, reps=reps, warm=5), 2)
+                    except GpgError:
+                        row[v] = None
+                check(lib.gpg_set_sor_variant(rs, g, -1))
+                rec = {"precision": f"f{8 * rs}", "ghost": g, "npatch": n, "us": row}
+                out.append(rec)
+                print(json.dumps(rec), flush=True)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--npatch", type=int, default=4096)
     ap.add_argument("--json", default=None)
     ap.add_argument("--no-write", action="store_true")
+    ap.add_argument("--sizes", default=None, help="report only: variant times at these patch counts")
+    ap.add_argument("--gravity", action="store_true", help="with --sizes: fused gravity update in each launch")
     a = ap.parse_args(argv)
+    if a.sizes:
+        rep = sizes_report([int(x) for x in a.sizes.split(",")], a.gravity)
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(rep, f, indent=1)
+        return 0
     rep = tune(a.npatch)
     if not a.no_write:
         path = os.path.join(HERE, "lib", "sor_tune.txt")

@@ -128,19 +128,21 @@ std::atomic<int> g_sor_variant[2][6] = {
 // file): every launch then uses it, whatever its size
 std::atomic<bool> g_sor_pinned[2][6] = {};
 // Small launches: at a few thousand patches and fewer a launch leaves SMs
-// short of teams, and the layouts that split each pair column between two
-// lanes (twice the threads per patch) finish each patch sooner.  Measured on
-// B200 at 64-4096 patches per launch (reference parameters, gravity on), the
-// variant below wins up to max_npatch patches: FP32 ghost 1 at 256 patches
-// 18.7 -> 13.2 us per launch, ghost 2 18.7 -> 12.5, ghost 5 at 2048 166 -> 145;
-// FP64 ghost 2 at 256 53.5 -> 39.1.  Beyond it the table above holds.
+// short of teams, and other layouts finish each patch sooner: those that split
+// each pair column between two lanes (twice the threads per patch), and for
+// FP64 ghost 4 the staged one.  Measured on B200 at 64-4096 patches per launch
+// (autotune.py --sizes, reference parameters, gravity on), the variant below
+// wins up to max_npatch patches: FP32 ghost 1 at 256 patches 19.7 -> 13.9 us
+// per launch, ghost 2 18.7 -> 12.7, ghost 3 at 2048 91.3 -> 84.0; FP64 ghost 2
+// at 256 53.6 -> 39.1, ghost 4 at 64 72.7 -> 59.6.  Beyond it the table above
+// holds.
 struct SorSmall {
   int max_npatch, variant;
 };
 constexpr SorSmall kSorSmall[2][6] = {
-    // ghost:  -       1          2          3         4           5
-    {{0, 0}, {2048, 6}, {2048, 6}, {2048, 7}, {256, 7}, {2048, 11}},   // float
-    {{0, 0}, {256, 8}, {256, 7}, {0, 0}, {0, 0}, {0, 0}},              // double
+    // ghost:  -       1          2          3         4          5
+    {{0, 0}, {2048, 6}, {2048, 6}, {2048, 7}, {256, 7}, {0, 0}},     // float
+    {{0, 0}, {256, 8}, {256, 7}, {0, 0}, {256, 14}, {0, 0}},         // double
 };
 std::once_flag g_tune_once;
 
