@@ -113,13 +113,13 @@ constexpr int kSorVariantSplit[kSorVariants] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2,
 constexpr int kSorVariantRows[kSorVariants] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2};   // rows per lane
 constexpr bool kSorVariantStaged[kSorVariants] = {false, false, false, false, false, false, false, false, false,
                                                   false, false, false, false, false, true,  true,  true};
-// atomic: gpg_set_sor_variant may run on one host thread while another launches
 constexpr int kSorDefault[2][6] = {
     // ghost:  -  1  2  3  4  5       (autotune.py on B200, 4096 patches, reference parameters;
     //                                  FP32 g4 / g5 and FP64 g5 confirmed by three A/B bench runs)
     {0, 10, 11, 10, 10, 15},   // float
     {0, 11, 13, 11, 10, 14},   // double
 };
+// atomic: gpg_set_sor_variant may run on one host thread while another launches
 std::atomic<int> g_sor_variant[2][6] = {
     {kSorDefault[0][0], kSorDefault[0][1], kSorDefault[0][2], kSorDefault[0][3], kSorDefault[0][4], kSorDefault[0][5]},
     {kSorDefault[1][0], kSorDefault[1][1], kSorDefault[1][2], kSorDefault[1][3], kSorDefault[1][4], kSorDefault[1][5]},
@@ -274,7 +274,8 @@ int prepare_staged_v() {
 // Set on the host thread that prepares and captures a concurrent batch plan:
 // its branches share the SMs, and a staged persistent kernel, whose CTAs take
 // patches at a fixed stride, then finishes with a tail (65,536 mixed patches:
-// 1.43 vs 1.34 ms per graph launch), so staged variants run as their unstaged layouts there.
+// 1.43 vs 1.34 ms per graph launch), so staged variants run as their unstaged
+// layouts there.
 thread_local bool t_shared_sms = false;
 struct SharedSms {
   SharedSms() { t_shared_sms = true; }
