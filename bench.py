@@ -862,7 +862,7 @@ def main(argv=None) -> int:
         from gpg.lib import check
         lib = library()
         v, z, y = C.c_int(), C.c_int(), C.c_int()
-        check(lib.gpg_get_sor_variant(p.real_size, p.ghost, C.byref(v)))
+        check(lib.gpg_sor_variant_for_launch(p.real_size, p.ghost, NPATCH, C.byref(v)))
         check(lib.gpg_sor_variant_layout(v.value, C.byref(z), C.byref(y)))
         m = 6 + 2 * p.ghost
         acc = (4.0 if y.value == 1 else 3.0) + (1.0 / (m // z.value) if z.value == 2 else 0.0)

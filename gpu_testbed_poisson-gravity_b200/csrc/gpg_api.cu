@@ -869,6 +869,14 @@ extern "C" int gpg_set_sor_variant(int real_size, int ghost, int variant) {
   return GPG_OK;
 }
 
+extern "C" int gpg_sor_variant_for_launch(int real_size, int ghost, int64_t npatch, int *variant) {
+  std::call_once(g_tune_once, load_tune_file);
+  if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || npatch < 0 || !variant)
+    return fail(GPG_ERR_INVALID, "real_size %d ghost %d npatch %lld", real_size, ghost, (long long)npatch);
+  *variant = sor_variant_for(real_size == 8, ghost, npatch);
+  return GPG_OK;
+}
+
 extern "C" int gpg_get_sor_variant(int real_size, int ghost, int *variant) {
   std::call_once(g_tune_once, load_tune_file);
   if ((real_size != 4 && real_size != 8) || ghost < 1 || ghost > 5 || !variant)

@@ -68,6 +68,7 @@ def library(path: str | None = None):
         "gpg_sor_variant_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "gpg_sor_variant_layout": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "gpg_sor_variant_staged": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+        "gpg_sor_variant_for_launch": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.POINTER(C.c_int)]),
         "gpg_sor_layout": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
         "gpg_set_sor_variant": (C.c_int, [C.c_int, C.c_int, C.c_int]),
         "gpg_get_sor_variant": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),

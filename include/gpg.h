@@ -284,6 +284,9 @@ GPG_API int gpg_sor_layout(int real_size, int ghost, int variant, int *fields);
 /* variant -1 returns (real_size, ghost) to the library's built-in choice */
 GPG_API int gpg_set_sor_variant(int real_size, int ghost, int variant);
 GPG_API int gpg_get_sor_variant(int real_size, int ghost, int *variant);
+/* the variant a solve of npatch patches (one launch) at (real_size, ghost)
+ * runs now: the small-launch or large-launch choice, or the one set */
+GPG_API int gpg_sor_variant_for_launch(int real_size, int ghost, int64_t npatch, int *variant);
 
 /* ---------------------------------------------------------------------------
  * Learned initial guess for ghost-size-1 SOR (GPG_INIT_GUESS).  No reference

@@ -107,3 +107,29 @@ def test_sor_variant_table_queries():
     after = C.c_int()
     check(lib.gpg_get_sor_variant(4, 3, C.byref(after)))
     assert after.value == before.value
+
+
+def test_launch_size_choice_of_sor_variants():
+    """Small launches take their own built-in variant until one is set; a set
+    variant holds at every size; -1 restores the library's choice."""
+    lib = library()
+    n = lib.gpg_sor_variant_count()
+    v = C.c_int()
+
+    def at(npatch):
+        check(lib.gpg_sor_variant_for_launch(4, 1, npatch, C.byref(v)))
+        return v.value
+
+    large = C.c_int()
+    check(lib.gpg_get_sor_variant(4, 1, C.byref(large)))
+    small = at(64)
+    assert at(1 << 20) == large.value and small != large.value
+    assert at(2048) == small and at(2049) == large.value
+    check(lib.gpg_set_sor_variant(4, 1, (large.value + 1) % n))
+    try:
+        assert at(64) == at(1 << 20) == (large.value + 1) % n
+    finally:
+        check(lib.gpg_set_sor_variant(4, 1, -1))
+    assert at(64) == small and at(1 << 20) == large.value
+    with pytest.raises(GpgError):
+        check(lib.gpg_sor_variant_for_launch(4, 1, -1, C.byref(v)))
