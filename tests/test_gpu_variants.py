@@ -43,3 +43,40 @@ def test_variants_bit_identical(rs, g):
     for v, *o in outs[1:]:
         for a, b in zip(o, outs[0][1:]):
             assert np.array_equal(a, b), f"variant {v}"
+
+
+@pytest.mark.parametrize("rs,g,npatch", [(4, 5, 4096), (8, 5, 4096), (8, 4, 200), (4, 1, 300), (4, 1, 5000)])
+def test_library_choice_by_launch_size_and_alignment(rs, g, npatch):
+    """Without a variant set, the library picks one per launch size (small- or
+    large-launch table, staged layouts among them); a staged choice given inputs
+    off the 16-byte alignment of its bulk copies runs its unstaged layout.
+    Every path returns the bits of variant 0."""
+    torch = pytest.importorskip("torch")
+    from gpg.lib import check, library, solve_device
+    lib = library()
+    dev = torch.device("cuda:0")
+    dt = np.float32 if rs == 4 else np.float64
+    d = make_patches(npatch, g, seed=700 + g, dtype=dt)
+    p = default_params(rs, g, GPG_SOR)
+    rho, pin, flu = (torch.from_numpy(d[k].copy()).to(dev) for k in ("rho", "pot_in", "flu"))
+
+    def shifted(t):
+        # the same values one element past a 16-byte boundary
+        buf = torch.empty(t.numel() + 1, dtype=t.dtype, device=dev)
+        buf[1:] = t.reshape(-1)
+        return buf[1:].view(t.shape)
+
+    check(lib.gpg_set_sor_variant(rs, g, -1))
+    chosen = C.c_int()
+    check(lib.gpg_sor_variant_for_launch(rs, g, npatch, C.byref(chosen)))
+    outs = [solve_device(p, rho, pin, flu=flu.clone()), solve_device(p, shifted(rho), shifted(pin), flu=flu.clone())]
+    check(lib.gpg_set_sor_variant(rs, g, 0))
+    try:
+        outs.append(solve_device(p, rho, pin, flu=flu.clone()))
+    finally:
+        check(lib.gpg_set_sor_variant(rs, g, -1))
+    torch.cuda.synchronize()
+    ref = [o.cpu() for o in outs[-1]]
+    for k, out in enumerate(outs[:-1]):
+        for a, b in zip(out, ref):
+            assert torch.equal(a.cpu(), b), (chosen.value, k)
