@@ -134,15 +134,18 @@ std::atomic<bool> g_sor_pinned[2][6] = {};
 // (autotune.py --sizes, reference parameters, gravity on), the variant below
 // wins up to max_npatch patches: FP32 ghost 1 at 256 patches 19.7 -> 13.9 us
 // per launch, ghost 2 18.7 -> 12.7, ghost 3 at 2048 91.3 -> 84.0; FP64 ghost 2
-// at 256 53.6 -> 39.1, ghost 4 at 64 72.7 -> 59.6.  Beyond it the table above
-// holds.
+// at 256 53.6 -> 39.1, ghost 4 at 64 72.7 -> 59.6.  FP64 ghost 5 keeps the
+// unstaged v11 up to 1024 patches: the staged kernel hands patches out at a
+// fixed stride, and 1024 patches over its 296 teams leave some teams a fourth
+// patch (333 vs 360 us; through the CUAPI path, 4 streams of 1024 patches,
+// 1.47 vs 1.55 ms of kernels per call).  Beyond it the table above holds.
 struct SorSmall {
   int max_npatch, variant;
 };
 constexpr SorSmall kSorSmall[2][6] = {
     // ghost:  -       1          2          3         4          5
     {{0, 0}, {2048, 6}, {2048, 6}, {2048, 7}, {256, 7}, {0, 0}},     // float
-    {{0, 0}, {256, 8}, {256, 7}, {0, 0}, {256, 14}, {0, 0}},         // double
+    {{0, 0}, {256, 8}, {256, 7}, {0, 0}, {256, 14}, {1024, 11}},     // double
 };
 std::once_flag g_tune_once;
 
