@@ -449,7 +449,7 @@ def default_case(torch, dev, cpu: bool) -> dict:
 
 
 def learned_config(torch):
-    """BASELINE's learned-guess configuration on 65536 held-out ghost-1 patches
+    """The learned-guess workload on 65536 held-out ghost-1 FP32 patches
     (rho0 log-uniform over 4 decades, power index uniform in [1.5, 2.5]), every
     start solved to the calibrated fixed residual: zero-start plain SOR (the
     metric's comparison), the interpolated start (the reference's), the
@@ -548,7 +548,8 @@ def learned_e2e(torch, steps: int) -> dict:
 
 
 def learned_vs_plain(rec: dict) -> dict:
-    """The comparison BASELINE's metric names, from learned_config()."""
+    """The headline comparison (learned-init + SOR vs plain zero-start SOR to
+    the fixed residual), from learned_config()."""
     if "learned_linear" not in rec:
         return {"unavailable": rec.get("unavailable", "no learned arm")}
     z, i, l = rec["plain_zero_start"], rec["plain_interpolated_start"], rec["learned_linear"]
