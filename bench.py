@@ -102,7 +102,12 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
+            # the timed region starts once samples flow (nvidia-smi takes a
+            # fraction of a second to start), so that it is covered
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            time.sleep(0.1)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
